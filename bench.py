@@ -1,0 +1,440 @@
+"""Throughput of the HEALPix SHT+iSHT on B200: maps/s at nside=1024, lmax=mmax=2047, batch 64.
+
+One step = analysis (SHT, with the configured Jacobi refinement) of a batch of
+64 float32 maps followed by synthesis (iSHT) of the resulting coefficients.
+Inputs are band-limited Gaussian fields (C_l ~ (l+1)^-2) plus N(0, 1e-3)
+white noise, generated on the device from a fixed seed; each batch is 3.2 GB,
+larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision bf16x3|tf32|fp32] [--refine k]
+  python bench.py --impl reference ...   # the reference's CPU algorithm (oracle port) on the host
+
+Under torchrun every rank runs its own batch (replicas, no collective on the
+data path); the timed region is bracketed by barriers and the max over ranks
+is reported.  Prints one JSON line on rank 0.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "SHT+iSHT maps/s nside1024 lmax2047 B64: mixed vs FP32 plain, err<=1e-5 vs FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hpx", choices=["hpx", "reference"])
+    ap.add_argument("--precision", default="auto")
+    ap.add_argument("--refine", type=int, default=-1, help="Jacobi iterations (-1: default for the precision)")
+    ap.add_argument("--nside", type=int, default=1024)
+    ap.add_argument("--lmax", type=int, default=2047)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
+    ap.add_argument("--cpu-sample-m", type=int, default=12)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": smax,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_baseline(nside, lmax, n_m, steps=1):
+    from oracle import hpx_oracle as O
+
+    cores = os.cpu_count() or 1
+    secs = []
+    for s in range(steps):
+        r = O.time_reference_sample(nside, lmax, lmax, n_m=n_m, seed=s, threads=cores)
+        secs.append(r["seconds_per_map"])
+    spm = statistics.median(secs)
+    return {
+        "value": 1.0 / spm,
+        "unit": "maps/s",
+        "cores": cores,
+        "kind": "port",
+        "sample": (
+            f"one float64 map at nside={nside}, L=M={lmax}: all ring rfft/irfft, and the reference's dense per-m "
+            f"Legendre contraction timed on {r['n_m']} sampled orders and scaled by M/{r['n_m']} (the full dense "
+            f"table is 68.6 GB); numpy with {cores} host threads"
+        ),
+        "seconds_per_map": spm,
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    lm = args.lmax
+    cores = os.cpu_count() or 1
+    from oracle import hpx_oracle as O
+
+    for w in range(args.warmup):
+        O.time_reference_sample(args.nside, lm, lm, n_m=max(2, args.cpu_sample_m // 4), seed=100 + w, threads=cores)
+    secs = []
+    for s in range(args.steps):
+        r = O.time_reference_sample(args.nside, lm, lm, n_m=args.cpu_sample_m, seed=s, threads=cores)
+        secs.append(r["seconds_per_map"])
+    total = sum(secs)
+    value = args.steps / total
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "maps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"SHT+iSHT nside={args.nside} lmax=mmax={lm}, one map per step (bounded sample)", "batch": 1},
+        "cpu_baseline": {
+            "value": value,
+            "unit": "maps/s",
+            "cores": cores,
+            "kind": "port",
+            "sample": f"per step one map: full ring FFTs + dense per-m Legendre contraction on {args.cpu_sample_m} sampled orders scaled by M",
+        },
+        "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU arm
+def make_inputs(torch, hpx, nside, L, B, device, seed=2):
+    """cfg3 maps: band-limited a_lm with C_l ~ (l+1)^-2 synthesised, plus N(0, 1e-3) noise."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    l = torch.arange(L, device=device, dtype=torch.float32)
+    sig = (1.0 / (l + 1.0))[:, None]
+    re = torch.randn((B, L, L), generator=g, device=device) * sig
+    im = torch.randn((B, L, L), generator=g, device=device) * sig
+    tri = torch.tril(torch.ones(L, L, device=device, dtype=torch.bool))
+    a = torch.complex(re, im) * tri
+    a[..., 0] = a[..., 0].real.to(a.dtype)
+    a = a / np.sqrt(2.0)
+    isht = hpx.iSHTCUDA(nside, lmax=L, mmax=L)
+    with torch.no_grad():
+        f = isht(a)
+    del a
+    f += torch.randn(f.shape, generator=g, device=device) * np.sqrt(1e-3)
+    return f.contiguous()
+
+
+def time_steps(torch, fn, steps, warmup, dist, stream):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms
+
+
+def run_gpu(args):
+    import torch
+
+    import cuhpx_b200 as hpx
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        dist = tdist
+
+    nside, L, B = args.nside, args.lmax, args.batch
+    prec = args.precision
+    if prec == "auto":
+        prec = "bf16x3" if _tc_available(hpx, dev) else "fp32"
+    refine = args.refine if args.refine >= 0 else (1 if prec in ("bf16x3", "tf32") else 0)
+
+    f = make_inputs(torch, hpx, nside, L, B, dev)
+    sht = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, refine_iters=refine)
+    isht = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+
+    def step():
+        with torch.no_grad():
+            a = sht(f)
+            out["f2"] = isht(a)
+
+    plan = hpx.get_plan(nside, L, L, "ring", prec, local)
+    clocks = ClockSampler(local)
+    # warm-up, then the timed region with per-kernel events and clock sampling
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    plan.stats_enable(True)
+    clocks.start()
+    ms = time_steps(torch, step, args.steps, 0, dist, stream)
+    clk = clocks.stop()
+    stats = plan.stats_read()
+    plan.stats_enable(False)
+    ms_step = ms / args.steps
+    value = world * B * args.steps / (ms / 1000.0)
+    launches_per_step = sum(v[0] for v in stats.values()) / args.steps
+
+    # roofline of the dominant kernel
+    roof = roofline(stats, args, prec, refine, nside, L, B)
+
+    # plain FP32 comparison (the target is >= 2x this on the same GPU)
+    plain = None
+    if not args.no_plain and prec != "fp32":
+        sht_p = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision="fp32")
+        isht_p = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision="fp32")
+
+        def step_p():
+            with torch.no_grad():
+                isht_p(sht_p(f))
+
+        ms_p = time_steps(torch, step_p, max(1, args.steps // 2), 1, dist, stream)
+        plain = world * B * max(1, args.steps // 2) / (ms_p / 1000.0)
+
+    # end to end through the public modules with host buffers
+    e2e = None
+    if not args.no_e2e:
+        fh = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+        fh.copy_(f)
+        oh = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+
+        def step_e2e():
+            with torch.no_grad():
+                x = fh.to(dev, non_blocking=True)
+                y = isht(sht(x))
+                oh.copy_(y, non_blocking=True)
+
+        ms_e = time_steps(torch, step_e2e, max(1, args.steps // 2), 1, dist, stream)
+        nb = f.numel() * f.element_size()
+        e2e = {"value": world * B * max(1, args.steps // 2) / (ms_e / 1000.0), "unit": "maps/s", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(nside, L, args.cpu_sample_m)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "maps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if prec == "fp32" else f"f32 io, {prec} contraction",
+            "data": "synthetic",
+            "config": {
+                "workload": f"SHT(refine={refine})+iSHT nside={nside} lmax=mmax={L} batch={B} per GPU",
+                "nside": nside,
+                "lmax": L,
+                "mmax": L,
+                "batch_per_gpu": B,
+                "precision": prec,
+                "refine_iters": refine,
+                "l2": "inputs larger than L2 (3.2 GB per batch); no flush",
+                "parallelism": f"replicas x{world}",
+            },
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "kernels_per_step": launches_per_step,
+            "stage_ms_per_step": {k: v[1] / args.steps for k, v in stats.items() if v[0]},
+            "roofline": roof,
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "plain_fp32_maps_per_s": plain,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _tc_available(hpx, dev):
+    try:
+        hpx.get_plan(8, 17, 17, "ring", "bf16x3", dev.index)
+        return True
+    except Exception:
+        return False
+
+
+def algorithmic(nside, L, M):
+    """Useful FLOPs of one Legendre contraction direction per map (folded, truncated)
+    and algorithmic bytes of one ring-FFT direction per map."""
+    flops = 0
+    NP = 2 * nside
+    for p in range(NP):
+        nphi = 4 * (p + 1) if p < nside - 1 else 4 * nside
+        mt = min(M, nphi // 2 + 1)
+        ms = np.arange(mt)
+        flops += 4 * int(np.sum(np.maximum(L - ms, 0)))
+    npix = 12 * nside * nside
+    kept = 0
+    for t in range(4 * nside - 1):
+        tn = t if t < NP else 4 * nside - 2 - t
+        nphi = 4 * (tn + 1) if tn < nside - 1 else 4 * nside
+        kept += min(M, nphi // 2 + 1)
+    fft_bytes = 4 * npix + 8 * kept
+    return flops, fft_bytes
+
+
+def roofline(stats, args, prec, refine, nside, L, B):
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    flops_map, fft_bytes_map = algorithmic(nside, L, L)
+    dom = max(stats.items(), key=lambda kv: kv[1][1])
+    name, (n, tot) = dom
+    per_launch_ms = tot / max(n, 1)
+    chunk = min(B, 64)
+    if name.startswith("legendre"):
+        useful = flops_map * chunk
+        if prec in ("bf16x3", "tf32"):
+            terms = 3 if prec == "bf16x3" else 1
+            peak = peaks.get("bf16_tflops", 1590.0) if prec == "bf16x3" else peaks.get("bf16_tflops", 1590.0) / 2
+            achieved = useful * terms / (per_launch_ms * 1e-3) / 1e12
+            return {
+                "kernel": name,
+                "bound": "tensor",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "traffic": None,
+                "useful_tflops": useful / (per_launch_ms * 1e-3) / 1e12,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" + ("; tf32 taken as half" if prec == "tf32" else ""),
+            }
+        achieved = useful / (per_launch_ms * 1e-3) / 1e12
+        peak = FP32_SIMT_PEAK_TFLOPS
+        return {
+            "kernel": name,
+            "bound": "fp32_simt",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "traffic": None,
+            "peak_source": "FMA-loop peak measured on this pool's B200 (profiles/peaks_fp32_fp64.md)",
+        }
+    byts = fft_bytes_map * chunk
+    achieved = byts / (per_launch_ms * 1e-3) / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None}
+
+
+# measured with an FMA loop on this pool's B200 (see profiles/peaks_fp32_fp64.md)
+FP32_SIMT_PEAK_TFLOPS = 72.0
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,20 @@
+"""hpx_b200: HEALPix spherical-harmonic transforms for NVIDIA B200 (sm_100a).
+
+Drop-in for the SHT path of cuHPX: ``SHTCUDA``, ``iSHTCUDA``, ``Grid`` and
+``Regridding``.  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
+C ABI in ``include/hpx_b200.h``); there is no CPU fallback.
+"""
+
+from . import sht_tools
+from .hpx_sht import Plan, SHTCUDA, SHTFunction, clear_plan_cache, get_plan, iSHTCUDA, iSHTFunction
+
+__all__ = [
+    "SHTCUDA",
+    "iSHTCUDA",
+    "SHTFunction",
+    "iSHTFunction",
+    "Plan",
+    "get_plan",
+    "clear_plan_cache",
+    "sht_tools",
+]

@@ -1,0 +1,85 @@
+"""Build the hpx_b200 CUDA library in-tree (``cuhpx_b200/libhpx_b200.so``).
+
+The library is one translation unit compiled by nvcc for sm_100a only and
+exports the C ABI declared in ``include/hpx_b200.h``.  Python reaches it
+through ctypes (``cuhpx_b200/_lib.py``); nothing here depends on torch.
+
+    python -m cuhpx_b200.build [--force] [--debug]
+"""
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libhpx_b200.so")
+SOURCES = ["hpx_plan.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps():
+    files = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
+    files.append(os.path.join(REPO, "include", "hpx_b200.h"))
+    files.append(os.path.abspath(__file__))
+    return files
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(f) <= t for f in _deps())
+
+
+def build(force=False, debug=False, verbose=False):
+    if not force and up_to_date():
+        return LIB
+    cmd = [
+        _nvcc(),
+        *ARCH,
+        "-O3",
+        "-lineinfo",
+        "-std=c++17",
+        "-shared",
+        "-Xcompiler",
+        "-fPIC,-fvisibility=hidden",
+        "-Xptxas",
+        "-v" if verbose else "-O3",
+        "--expt-relaxed-constexpr",
+        "-I",
+        os.path.join(REPO, "include"),
+        "-o",
+        LIB + ".tmp",
+        *[os.path.join(CSRC, s) for s in SOURCES],
+        "-lcuda",
+    ]
+    if debug:
+        cmd.insert(1, "-DHPX_CHECK_BOUNDS=1")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libhpx_b200.so")
+    if verbose:
+        sys.stderr.write(res.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--debug", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, debug=a.debug, verbose=a.verbose))

@@ -1,0 +1,104 @@
+// Shared device/host helpers of the hpx_b200 library: HEALPix ring geometry,
+// complex arithmetic, status plumbing.
+//
+// Ring geometry restates cuhpx/sht_tools.py:161-189, 319-332 (nphi_ring,
+// cumulative_nphi_ring, p2phi_ring) and the z formula of
+// cuhpx/sht_tools.py:114-140.  Rings are numbered t = 0 .. 4*nside-2 from north
+// to south; ring t and ring 4*nside-2-t are mirror images (z -> -z), the
+// equator is t = 2*nside-1.  "Ring pair" p in [0, 2*nside) names the north ring
+// t=p and its mirror (the equator pairs with itself).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define HPX_HD __host__ __device__ __forceinline__
+
+namespace hpx {
+
+// ------------------------------------------------------------------ geometry
+HPX_HD int nrings(int nside) { return 4 * nside - 1; }
+HPX_HD int64_t npix(int nside) { return 12ll * nside * nside; }
+
+// pixels on ring t
+HPX_HD int ring_nphi(int t, int nside) {
+    if (t < nside - 1) return 4 * (t + 1);
+    if (t <= 3 * nside - 1) return 4 * nside;
+    return 4 * (4 * nside - t - 1);
+}
+
+// first pixel of ring t (RING order)
+HPX_HD int64_t ring_start(int t, int nside) {
+    if (t < nside) return 2ll * t * (t + 1);
+    if (t < 3 * nside) return 2ll * nside * (nside + 1) + (int64_t)(t - nside) * 4 * nside;
+    int64_t r = 4 * nside - t - 1;
+    return 12ll * nside * nside - 2 * r * (r + 1);
+}
+
+// phi0 of ring t is s*pi/nphi with s in {0,1} (cuhpx/sht_tools.py:161-176):
+// polar rings always have s=1, equatorial rings alternate.
+HPX_HD int ring_shift(int t, int nside) {
+    if (t + 1 >= nside && t + 1 <= 3 * nside) return (t - nside + 2) & 1;
+    return 1;
+}
+
+// z = cos(theta) of ring t, exact formula in double
+HPX_HD double ring_z(int t, int nside) {
+    double n = (double)nside;
+    if (t < nside - 1) {
+        double a = (double)(t + 1);
+        return 1.0 - a * a / (3.0 * n * n);
+    }
+    if (t <= 3 * nside - 1) return 4.0 / 3.0 - 2.0 * (double)(t + 1) / (3.0 * n);
+    double a = (double)(4 * nside - 1 - t);
+    return a * a / (3.0 * n * n) - 1.0;
+}
+
+// sin^2(theta) of ring t computed without cancellation near the poles
+HPX_HD double ring_sin2(int t, int nside) {
+    double n = (double)nside;
+    int tn = t < 2 * nside ? t : 4 * nside - 2 - t;  // north-hemisphere ring
+    if (tn < nside - 1) {
+        double a = (double)(tn + 1);
+        double omz = a * a / (3.0 * n * n);  // 1 - z
+        return omz * (2.0 - omz);
+    }
+    double z = ring_z(tn, nside);
+    return (1.0 - z) * (1.0 + z);
+}
+
+// the first north ring that carries order m: F_m(t) is kept only for
+// m <= nphi_t/2 (cuhpx/hpx_sht.py:47-48 truncates at min(L, nphi/2+1))
+HPX_HD int first_ring_for_m(int m, int nside) {
+    if (m > 2 * nside) return 2 * nside;  // no ring carries this order
+    // polar ring t has nphi = 4(t+1): need 2(t+1) >= m
+    int t = (m + 1) / 2 - 1;
+    if (t < 0) t = 0;
+    if (t > nside - 1) t = nside - 1;  // equatorial rings carry m <= 2*nside
+    return t;
+}
+
+// ------------------------------------------------------------------ complex
+template <typename T>
+struct __align__(2 * sizeof(T)) cplx {
+    T re, im;
+};
+
+template <typename T>
+HPX_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+HPX_HD cplx<T> cmulc(cplx<T> a, cplx<T> b) {  // a * conj(b)
+    return {a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im};
+}
+template <typename T>
+HPX_HD cplx<T> cadd(cplx<T> a, cplx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T>
+HPX_HD cplx<T> csub(cplx<T> a, cplx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T>
+HPX_HD cplx<T> cconj(cplx<T> a) { return {a.re, -a.im}; }
+template <typename T>
+HPX_HD cplx<T> cscale(cplx<T> a, T s) { return {a.re * s, a.im * s}; }
+
+}  // namespace hpx

@@ -1,0 +1,615 @@
+// hpx_b200 plan object and C ABI (see include/hpx_b200.h).
+//
+// A plan owns, on one device: the ring-pair table (geometry, quadrature
+// weight, Bluestein sizes), FFT twiddles, the Bluestein chirp spectra and the
+// per-(m, ring) Legendre start values.  It replaces the reference's
+// construction-time precompute (cuhpx/hpx_sht.py:645-683: FITS weights, the
+// dense FP64 legpoly_torch table built by an O(L^2) Python loop, W) and its
+// process-global cuFFT plan singletons (src/harmonic_transform/hpx_fft.h:69-255,
+// hpx_fft.cpp:49,125), which were neither thread-safe nor batch-size
+// independent.  Plans here are immutable after creation; every call brings its
+// own workspace, so calls on different streams with different workspaces may
+// run concurrently.
+//
+// Adjoints (exact, w.r.t. <x,y> = sum x*y on maps and Re sum conj(a)*b on alm):
+//   forward  a = P^T W F f  ->  adjoint  f_bar = F^H W P a_bar
+//     where F^H of the truncated, phase-shifted real DFT is the inverse ring
+//     transform with the m = 0 and m = nphi/2 terms weighted 1 and all other
+//     orders weighted 1/2 (the irfft counts them twice);
+//   inverse  f = F^{-1} P a  ->  adjoint a_bar = P^T c F f_bar
+//     with c_m = 2 for 0 < m < nphi/2 and 1 for m = 0, nphi/2.
+// The reference's hand-written backward (cuhpx/hpx_sht.py:565-583, 614-641)
+// halves the m = 0 term and mishandles the ring Nyquist terms; these do not.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/hpx_b200.h"
+#include "hpx_kernels.cuh"
+#include "legendre_tc.cuh"
+
+using namespace hpx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define HPX_CUDA_TRY(expr)                                                                            \
+    do {                                                                                              \
+        cudaError_t _e = (expr);                                                                      \
+        if (_e != cudaSuccess)                                                                        \
+            return set_err(_e == cudaErrorMemoryAllocation ? HPX_ERR_OOM : HPX_ERR_CUDA,              \
+                           std::string(#expr) + ": " + cudaGetErrorString(_e));                      \
+    } while (0)
+
+int ilog2_exact(int v) {
+    if (v <= 0 || (v & (v - 1))) return -1;
+    int r = 0;
+    while ((1 << r) < v) ++r;
+    return r;
+}
+int ceil_log2(int v) {
+    int r = 0;
+    while ((1 << r) < v) ++r;
+    return r;
+}
+
+enum Stage { kStRingFwd = 0, kStRingInv, kStLegFwd, kStLegInv, kStAlmCols, kNumStages };
+const char* kStageNames[kNumStages] = {"ring_fft_forward", "ring_fft_inverse", "legendre_forward",
+                                       "legendre_inverse", "alm_to_columns"};
+
+}  // namespace
+
+struct hpx_plan_s {
+    hpx_desc_t desc{};
+    int device = 0;
+    int nside = 0, L = 0, M = 0, NP = 0, R = 0;
+    int64_t npix = 0;
+    int prec = HPX_PREC_FP32;
+    bool f64 = false;
+    int batch_chunk = 64;
+    int logPmax = 0;
+    int bufP = 0;   // complex slots of the ring FFT buffer
+    int mtmax = 0;  // max orders per ring
+    int nmax = 0;   // max nphi
+    std::vector<RingPair> h_pairs;
+    RingPair* d_pairs = nullptr;
+    void* d_tw = nullptr;   // cplx<T> twiddles for the plan's FFT type
+    void* d_gtab = nullptr; // cplx<T> chirp spectra
+    int* d_lstart = nullptr;
+    double2* d_pstart = nullptr;
+    int2* d_invwork = nullptr;
+    int n_invwork = 0;
+    size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
+    TcPlan tc;  // tensor-core contraction state (mixed precision plans)
+
+    // per-kernel event timing (hpx_stats_*)
+    struct EvRec {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::mutex stats_mu;
+    bool stats_on = false;
+    std::vector<EvRec> stats_recs;
+    std::vector<cudaEvent_t> ev_pool;
+    int64_t stat_launch[kNumStages] = {};
+    double stat_ms[kNumStages] = {};
+
+    cudaEvent_t take_event() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+
+    ~hpx_plan_s() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        cudaFree(d_pairs);
+        cudaFree(d_tw);
+        cudaFree(d_gtab);
+        cudaFree(d_lstart);
+        cudaFree(d_pstart);
+        cudaFree(d_invwork);
+        tc_release(tc);
+        for (auto& r : stats_recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        cudaSetDevice(prev);
+    }
+
+    size_t real_size() const { return f64 ? sizeof(double) : sizeof(float); }
+    int cols() const { return ((2 * batch_chunk) + 3) & ~3; }
+    size_t spec_bytes() const { return (size_t)M * 2 * NP * cols() * real_size(); }
+    size_t almT_bytes() const { return (size_t)M * L * cols() * real_size(); }
+    size_t resid_bytes() const { return (size_t)batch_chunk * npix * real_size(); }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+int create_typed(hpx_plan_s* P) {
+    using C = cplx<T>;
+    const int Pmax = 1 << P->logPmax;
+    HPX_CUDA_TRY(cudaMalloc(&P->d_tw, (size_t)(Pmax / 2) * sizeof(C)));
+    k_twiddles<T><<<(Pmax / 2 + 255) / 256, 256>>>((C*)P->d_tw, Pmax);
+    HPX_CUDA_TRY(cudaGetLastError());
+    // chirp spectra computed in FP64 with FP64 twiddles
+    int64_t gsize = 0;
+    for (auto& rp : P->h_pairs)
+        if (rp.logh < 0) gsize = std::max<int64_t>(gsize, rp.gtab_off + (1ll << rp.logP));
+    if (gsize > 0) {
+        cplx<double>* tw64 = nullptr;
+        HPX_CUDA_TRY(cudaMalloc(&tw64, (size_t)(Pmax / 2) * sizeof(cplx<double>)));
+        k_twiddles<double><<<(Pmax / 2 + 255) / 256, 256>>>(tw64, Pmax);
+        HPX_CUDA_TRY(cudaMalloc(&P->d_gtab, (size_t)gsize * sizeof(C)));
+        size_t sm = (size_t)Pmax * sizeof(cplx<double>);
+        if (sm > 48 * 1024)
+            HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_chirp_spectra<T><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab);
+        cudaError_t e = cudaGetLastError();
+        cudaError_t e2 = cudaDeviceSynchronize();
+        cudaFree(tw64);
+        if (e != cudaSuccess || e2 != cudaSuccess)
+            return set_err(HPX_ERR_CUDA, std::string("chirp spectra: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    // shared memory budgets
+    P->ring_smem = ring_smem_bytes<T>(P->bufP, P->mtmax, P->nmax);
+    P->fwd_smem = fwd_smem_bytes<T>(P->L, P->nside);
+    P->inv_smem = inv_smem_bytes<T>(P->L);
+    int dev_max = 0;
+    HPX_CUDA_TRY(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
+    if ((int)P->ring_smem > dev_max || (int)P->fwd_smem > dev_max || (int)P->inv_smem > dev_max)
+        return set_err(HPX_ERR_UNSUPPORTED, "nside/lmax too large for the shared-memory kernels of this precision");
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->ring_smem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->ring_smem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->fwd_smem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->inv_smem));
+    return HPX_OK;
+}
+
+int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
+    P->desc = *d;
+    P->desc.ring_weights = nullptr;
+    P->device = d->device;
+    P->nside = d->nside;
+    P->L = d->lmax;
+    P->M = d->mmax;
+    P->NP = 2 * d->nside;
+    P->R = 4 * d->nside - 1;
+    P->npix = 12ll * d->nside * d->nside;
+    P->prec = d->precision;
+    P->f64 = d->precision == HPX_PREC_FP64;
+    P->batch_chunk = d->batch_chunk > 0 ? d->batch_chunk : 64;
+    const int N = P->nside;
+
+    // ---- ring pairs
+    P->h_pairs.resize(P->NP);
+    int64_t goff = 0;
+    int logPmax = 1, bufP = 2, mtmax = 0;
+    const double four_pi_over_npix = 4.0 * M_PI / (double)P->npix;
+    for (int p = 0; p < P->NP; ++p) {
+        RingPair& rp = P->h_pairs[p];
+        const int ts = 4 * N - 2 - p;
+        rp.nphi = ring_nphi(p, N);
+        rp.h = rp.nphi / 2;
+        rp.mt = std::min(P->M, rp.h + 1);
+        rp.shift_n = ring_shift(p, N);
+        rp.shift_s = ring_shift(ts, N);
+        rp.has_south = p != 2 * N - 1;
+        rp.start_n = ring_start(p, N);
+        rp.start_s = ring_start(ts, N);
+        rp.z = ring_z(p, N);
+        // quadrature weight (cuhpx/sht_tools.py:47-59): north ring index p+1
+        if (d->ring_weights) rp.w = four_pi_over_npix * (1.0 + d->ring_weights[p]);
+        else rp.w = four_pi_over_npix;
+        rp.logh = ilog2_exact(rp.h);
+        if (rp.logh >= 0) {
+            rp.logP = 0;
+            rp.gtab_off = -1;
+            logPmax = std::max(logPmax, std::max(rp.logh, 1));
+            bufP = std::max(bufP, rp.h);
+        } else {
+            rp.logP = ceil_log2(2 * rp.h - 1);
+            rp.gtab_off = goff;
+            goff += 1ll << rp.logP;
+            logPmax = std::max(logPmax, rp.logP);
+            bufP = std::max(bufP, 1 << rp.logP);
+        }
+        mtmax = std::max(mtmax, rp.mt);
+    }
+    P->logPmax = logPmax;
+    P->bufP = bufP;
+    P->mtmax = mtmax;
+    P->nmax = 4 * N;
+
+    HPX_CUDA_TRY(cudaMalloc(&P->d_pairs, sizeof(RingPair) * P->NP));
+    HPX_CUDA_TRY(cudaMemcpy(P->d_pairs, P->h_pairs.data(), sizeof(RingPair) * P->NP, cudaMemcpyHostToDevice));
+
+    // ---- Legendre start values
+    std::vector<double> logc(P->M);
+    long double acc = -0.5L * std::log2(4.0L * (long double)M_PI);
+    for (int m = 0; m < P->M; ++m) {
+        if (m > 0) acc += 0.5L * std::log2((2.0L * m + 1.0L) / (2.0L * m));
+        logc[m] = (double)acc;
+    }
+    double* d_logc = nullptr;
+    HPX_CUDA_TRY(cudaMalloc(&d_logc, sizeof(double) * P->M));
+    HPX_CUDA_TRY(cudaMemcpy(d_logc, logc.data(), sizeof(double) * P->M, cudaMemcpyHostToDevice));
+    const int64_t nms = (int64_t)P->M * P->NP;
+    HPX_CUDA_TRY(cudaMalloc(&P->d_lstart, sizeof(int) * nms));
+    HPX_CUDA_TRY(cudaMalloc(&P->d_pstart, sizeof(double2) * nms));
+    k_legendre_start<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, N, P->d_pairs, d_logc, P->d_lstart,
+                                                           P->d_pstart);
+    cudaError_t e = cudaGetLastError();
+    cudaError_t e2 = cudaDeviceSynchronize();
+    cudaFree(d_logc);
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return set_err(HPX_ERR_CUDA, std::string("legendre start: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+
+    // ---- inverse work list: (m, ring block), heaviest first
+    std::vector<int2> work;
+    const int RBI = InvCfg<float>::RBI;
+    for (int m = 0; m < P->M; ++m) {
+        const int t0 = first_ring_for_m(m, N);
+        const int K = P->NP - t0;
+        for (int rb = 0; rb < K; rb += RBI) work.push_back(make_int2(m, rb));
+    }
+    P->n_invwork = (int)work.size();
+    if (P->n_invwork > 0) {
+        HPX_CUDA_TRY(cudaMalloc(&P->d_invwork, sizeof(int2) * work.size()));
+        HPX_CUDA_TRY(cudaMemcpy(P->d_invwork, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice));
+    }
+
+    int rc = P->f64 ? create_typed<double>(P) : create_typed<float>(P);
+    if (rc != HPX_OK) return rc;
+    if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
+        rc = tc_create(P->tc, P->prec, P->nside, P->L, P->M, P->batch_chunk, P->device);
+        if (rc != HPX_OK) return set_err(rc, std::string("tensor-core plan: ") + tc_last_error());
+    }
+    return HPX_OK;
+}
+
+int check_call(hpx_plan_t plan, const void* a, const void* b, int64_t batch, void* ws, size_t ws_bytes) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    if (batch < 0) return set_err(HPX_ERR_INVALID_ARG, "negative batch");
+    if (batch == 0) return HPX_OK;
+    if (!a || !b) return set_err(HPX_ERR_INVALID_ARG, "null data pointer");
+    size_t need = 0;
+    hpx_workspace_size(plan, batch, &need);
+    if (!ws || ws_bytes < need)
+        return set_err(HPX_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes, got " +
+                                              std::to_string(ws_bytes));
+    if (((uintptr_t)ws & 255) != 0) return set_err(HPX_ERR_INVALID_ARG, "workspace must be 256-byte aligned");
+    return HPX_OK;
+}
+
+template <typename T>
+struct Pipeline {
+    const hpx_plan_s* P;
+    cudaStream_t st;
+    T* spec;
+    T* almT;
+    T* resid;
+
+    Pipeline(const hpx_plan_s* p, void* ws, cudaStream_t s) : P(p), st(s) {
+        char* c = (char*)ws;
+        spec = (T*)c;
+        c += (P->spec_bytes() + 255) & ~(size_t)255;
+        almT = (T*)c;
+        c += (P->almT_bytes() + 255) & ~(size_t)255;
+        resid = (T*)c;
+    }
+
+    int maps_per_cta(int nb) const { return std::min(nb, 4); }
+
+    // brackets one launch with events when the plan's stats are enabled
+    struct Timer {
+        hpx_plan_s* P;
+        cudaStream_t st;
+        int stage;
+        cudaEvent_t a = nullptr;
+        Timer(const hpx_plan_s* p, cudaStream_t s, int stg) : P(const_cast<hpx_plan_s*>(p)), st(s), stage(stg) {
+            if (!P->stats_on) return;
+            std::lock_guard<std::mutex> g(P->stats_mu);
+            a = P->take_event();
+            cudaEventRecord(a, st);
+        }
+        ~Timer() {
+            if (!a) return;
+            std::lock_guard<std::mutex> g(P->stats_mu);
+            cudaEvent_t b = P->take_event();
+            cudaEventRecord(b, st);
+            P->stats_recs.push_back({stage, a, b});
+        }
+    };
+
+    void ring_fwd(const T* map, int nb, int mode) {
+        const int g = maps_per_cta(nb);
+        dim3 grid(P->NP, (nb + g - 1) / g);
+        Timer tm(P, st, kStRingFwd);
+        k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, spec, P->cols(), P->nside, P->mtmax, P->bufP,
+                                                      P->d_pairs, (const cplx<T>*)P->d_tw, P->logPmax,
+                                                      (const cplx<T>*)P->d_gtab, mode);
+    }
+    void ring_inv(T* map, int nb, int mode, const T* ref) {
+        const int g = maps_per_cta(nb);
+        dim3 grid(P->NP, (nb + g - 1) / g);
+        Timer tm(P, st, kStRingInv);
+        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(spec, P->cols(), map, nb, g, P->nside, P->mtmax, P->bufP,
+                                                      P->d_pairs, (const cplx<T>*)P->d_tw, P->logPmax,
+                                                      (const cplx<T>*)P->d_gtab, mode, ref);
+    }
+    void leg_fwd(T* alm, int nb, int accumulate) {
+        const int C = P->cols();
+        Timer tm(P, st, kStLegFwd);
+        if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
+            tc_forward(P->tc, (const float*)spec, C, nb, (float*)alm, P->L, P->M, P->nside, P->d_pairs, P->d_lstart,
+                       P->d_pstart, accumulate, st);
+            return;
+        }
+        dim3 grid(P->M, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
+        k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->nside, P->d_pairs,
+                                                          P->d_lstart, P->d_pstart, accumulate);
+    }
+    void leg_inv(const T* alm, int nb) {
+        const int C = P->cols();
+        dim3 tg((P->M + 31) / 32, P->L, (nb + 15) / 16);
+        {
+            Timer tm(P, st, kStAlmCols);
+            k_alm_to_cols<T><<<tg, dim3(32, 8), 0, st>>>(alm, nb, P->L, P->M, almT, C);
+        }
+        Timer tm(P, st, kStLegInv);
+        if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
+            tc_inverse(P->tc, (const float*)almT, C, (float*)spec, P->L, P->M, P->nside, P->d_pairs, P->d_lstart,
+                       P->d_pstart, P->d_invwork, P->n_invwork, st);
+            return;
+        }
+        if (P->n_invwork == 0) return;
+        dim3 grid(P->n_invwork, (C + InvCfg<T>::CT - 1) / InvCfg<T>::CT);
+        k_leg_inv_simt<T><<<grid, 256, P->inv_smem, st>>>(almT, C, spec, P->L, P->M, P->nside, P->d_pairs,
+                                                          P->d_lstart, P->d_pstart, P->d_invwork);
+    }
+};
+
+enum Op { kForward, kInverse, kForwardAdjoint, kInverseAdjoint, kForwardRefined };
+
+template <typename T>
+int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void* ws, cudaStream_t st, int iters) {
+    Pipeline<T> pl(P, ws, st);
+    const int64_t bc = P->batch_chunk;
+    const size_t alm_stride = (size_t)P->L * P->M * 2;
+    for (int64_t b0 = 0; b0 < batch; b0 += bc) {
+        const int nb = (int)std::min<int64_t>(bc, batch - b0);
+        switch (op) {
+            case kForward:
+            case kInverseAdjoint: {
+                const T* map = (const T*)in + b0 * P->npix;
+                T* alm = (T*)out + b0 * alm_stride;
+                pl.ring_fwd(map, nb, op == kForward ? kRingPlain : kRingAdjoint);
+                pl.leg_fwd(alm, nb, 0);
+                break;
+            }
+            case kForwardRefined: {
+                // a = S f;  repeat: r = f - I a;  a += S r
+                const T* map = (const T*)in + b0 * P->npix;
+                T* alm = (T*)out + b0 * alm_stride;
+                pl.ring_fwd(map, nb, kRingPlain);
+                pl.leg_fwd(alm, nb, 0);
+                for (int it = 0; it < iters; ++it) {
+                    pl.leg_inv(alm, nb);
+                    pl.ring_inv(pl.resid, nb, kRingResidual, map);
+                    pl.ring_fwd(pl.resid, nb, kRingPlain);
+                    pl.leg_fwd(alm, nb, 1);
+                }
+                break;
+            }
+            case kInverse:
+            case kForwardAdjoint: {
+                const T* alm = (const T*)in + b0 * alm_stride;
+                T* map = (T*)out + b0 * P->npix;
+                pl.leg_inv(alm, nb);
+                pl.ring_inv(map, nb, op == kInverse ? kRingPlain : kRingAdjoint, nullptr);
+                break;
+            }
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(HPX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    return HPX_OK;
+}
+
+int dispatch(hpx_plan_t plan, Op op, const void* in, void* out, int64_t batch, void* ws, size_t ws_bytes,
+             void* stream, int iters = 0) {
+    int rc = check_call(plan, in, out, batch, ws, ws_bytes);
+    if (rc != HPX_OK || batch == 0) return rc;
+    DeviceGuard g(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        return plan->f64 ? run_op<double>(plan, op, in, out, batch, ws, st, iters)
+                         : run_op<float>(plan, op, in, out, batch, ws, st, iters);
+    } catch (const std::exception& ex) {
+        return set_err(HPX_ERR_CUDA, ex.what());
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan) {
+    if (!desc || !plan) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    *plan = nullptr;
+    if (desc->nside < 1 || desc->nside > 8192) return set_err(HPX_ERR_INVALID_ARG, "nside must be in [1, 8192]");
+    if (desc->lmax < 1 || desc->mmax < 1) return set_err(HPX_ERR_INVALID_ARG, "lmax and mmax must be >= 1");
+    if (desc->lmax > 65536 || desc->mmax > 65536) return set_err(HPX_ERR_INVALID_ARG, "lmax/mmax too large");
+    if (desc->precision < HPX_PREC_FP32 || desc->precision > HPX_PREC_TF32)
+        return set_err(HPX_ERR_INVALID_ARG, "unknown precision");
+    if (desc->batch_chunk < 0 || desc->batch_chunk > 4096) return set_err(HPX_ERR_INVALID_ARG, "batch_chunk out of range");
+    if (desc->refine_iters < 0 || desc->refine_iters > 64) return set_err(HPX_ERR_INVALID_ARG, "refine_iters out of range");
+    if (desc->flags != 0) return set_err(HPX_ERR_INVALID_ARG, "flags must be 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(HPX_ERR_CUDA, "no CUDA device");
+    }
+    if (desc->device < 0 || desc->device >= ndev) return set_err(HPX_ERR_INVALID_ARG, "bad device ordinal");
+    hpx_plan_s* P = new (std::nothrow) hpx_plan_s();
+    if (!P) return set_err(HPX_ERR_OOM, "host allocation failed");
+    DeviceGuard g(desc->device);
+    int rc;
+    try {
+        rc = plan_create(desc, P);
+    } catch (const std::bad_alloc&) {
+        rc = set_err(HPX_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& ex) {
+        rc = set_err(HPX_ERR_CUDA, ex.what());
+    }
+    if (rc != HPX_OK) {
+        delete P;
+        return rc;
+    }
+    *plan = P;
+    return HPX_OK;
+}
+
+int hpx_plan_destroy(hpx_plan_t plan) {
+    if (!plan) return HPX_OK;
+    delete plan;
+    return HPX_OK;
+}
+
+int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
+    if (!plan || !bytes) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    (void)batch;  // the batch is processed in chunks of batch_chunk maps
+    size_t s = ((plan->spec_bytes() + 255) & ~(size_t)255) + ((plan->almT_bytes() + 255) & ~(size_t)255) +
+               ((plan->resid_bytes() + 255) & ~(size_t)255);
+    s += tc_workspace_bytes(plan->tc);
+    *bytes = s;
+    return HPX_OK;
+}
+
+int hpx_sht_forward(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* ws, size_t ws_bytes,
+                    void* stream) {
+    return dispatch(plan, kForward, map, alm, batch, ws, ws_bytes, stream);
+}
+int hpx_sht_inverse(hpx_plan_t plan, const void* alm, void* map, int64_t batch, void* ws, size_t ws_bytes,
+                    void* stream) {
+    return dispatch(plan, kInverse, alm, map, batch, ws, ws_bytes, stream);
+}
+int hpx_sht_forward_refined(hpx_plan_t plan, const void* map, void* alm, int64_t batch, int32_t iters, void* ws,
+                            size_t ws_bytes, void* stream) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    if (iters < 0) iters = plan->desc.refine_iters;
+    if (iters > 64) return set_err(HPX_ERR_INVALID_ARG, "iters out of range");
+    return dispatch(plan, kForwardRefined, map, alm, batch, ws, ws_bytes, stream, iters);
+}
+int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_grad, int64_t batch, void* ws,
+                            size_t ws_bytes, void* stream) {
+    return dispatch(plan, kForwardAdjoint, alm_grad, map_grad, batch, ws, ws_bytes, stream);
+}
+int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, void* ws,
+                            size_t ws_bytes, void* stream) {
+    return dispatch(plan, kInverseAdjoint, map_grad, alm_grad, batch, ws, ws_bytes, stream);
+}
+
+int hpx_stats_enable(hpx_plan_t plan, int enable) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    std::lock_guard<std::mutex> g(plan->stats_mu);
+    plan->stats_on = enable != 0;
+    if (enable) {
+        for (int i = 0; i < kNumStages; ++i) {
+            plan->stat_launch[i] = 0;
+            plan->stat_ms[i] = 0.0;
+        }
+    }
+    return HPX_OK;
+}
+
+int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stages, int* n_stages) {
+    if (!plan || (!out && max_stages > 0)) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    DeviceGuard dg(plan->device);
+    std::lock_guard<std::mutex> g(plan->stats_mu);
+    for (auto& r : plan->stats_recs) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(r.b) != cudaSuccess || cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess)
+            return set_err(HPX_ERR_CUDA, "event timing failed");
+        plan->stat_launch[r.stage] += 1;
+        plan->stat_ms[r.stage] += ms;
+        plan->ev_pool.push_back(r.a);
+        plan->ev_pool.push_back(r.b);
+    }
+    plan->stats_recs.clear();
+    const int n = std::min(max_stages, (int)kNumStages);
+    for (int i = 0; i < n; ++i) {
+        out[i].name = kStageNames[i];
+        out[i].launches = plan->stat_launch[i];
+        out[i].total_ms = plan->stat_ms[i];
+    }
+    for (int i = 0; i < kNumStages; ++i) {
+        plan->stat_launch[i] = 0;
+        plan->stat_ms[i] = 0.0;
+    }
+    if (n_stages) *n_stages = kNumStages;
+    return HPX_OK;
+}
+
+int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    if (nside) *nside = plan->nside;
+    if (lmax) *lmax = plan->L;
+    if (mmax) *mmax = plan->M;
+    if (precision) *precision = plan->prec;
+    return HPX_OK;
+}
+
+const char* hpx_last_error(hpx_plan_t) { return g_last_error.c_str(); }
+
+const char* hpx_status_string(int status) {
+    switch (status) {
+        case HPX_OK: return "ok";
+        case HPX_ERR_INVALID_ARG: return "invalid argument";
+        case HPX_ERR_OOM: return "out of memory";
+        case HPX_ERR_CUDA: return "CUDA error";
+        case HPX_ERR_TIMEOUT: return "timeout";
+        case HPX_ERR_UNSUPPORTED: return "unsupported";
+        case HPX_ERR_WORKSPACE: return "workspace too small";
+        default: return "unknown status";
+    }
+}
+
+const char* hpx_version(void) { return "hpx_b200 0.1.0 (sm_100a)"; }
+
+}  // extern "C"

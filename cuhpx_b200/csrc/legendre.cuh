@@ -1,0 +1,390 @@
+// Associated-Legendre recurrence and the SIMT Legendre contractions.
+//
+// Pbar_l^m(x) is the orthonormal associated Legendre function without the
+// Condon-Shortley phase, as built by legpoly / legpoly_torch
+// (cuhpx/sht_tools.py:192-256):
+//   Pbar_m^m     = sqrt((2m+1)/(2m)) sin(theta) Pbar_{m-1}^{m-1},  Pbar_0^0 = 1/sqrt(4 pi)
+//   Pbar_{m+1}^m = sqrt(2m+3) x Pbar_m^m
+//   Pbar_l^m     = a_lm x Pbar_{l-1}^m - b_lm Pbar_{l-2}^m
+// The reference tabulates it densely ([M, L, rings], 68.6 GB in FP32 at
+// nside=1024, L=M=2047) and contracts with torch.einsum
+// (cuhpx/hpx_sht.py:557, 599).  Here nothing is tabulated: the plan stores,
+// per (m, north ring), the first degree l_s whose value is above 2^-600 and the
+// FP64 pair (Pbar_{l_s}, Pbar_{l_s+1}) -- found by an exponent-scaled FP64
+// recurrence so that the high-m polar seeds never underflow -- and every
+// contraction kernel runs the recurrence in FP64 on the fly from there.  Values
+// with l < l_s are below 2^-600 and are taken as 0.
+//
+// North/south symmetry: Pbar_l^m(-x) = (-1)^{l+m} Pbar_l^m(x), so a degree l
+// with l-m even contracts against S = w(F_t + F_t') and l-m odd against
+// D = w(F_t - F_t'); the sums run over the 2*nside north rings only.
+#pragma once
+
+#include "ring_fft.cuh"
+
+namespace hpx {
+
+// Three-term coefficients with the operation order of cuhpx/sht_tools.py:250-251
+// (IEEE double division and square root, so they equal the reference's bitwise).
+__device__ __forceinline__ double rec_a(int l, int m) {
+    double dl = l, dm = m;
+    return sqrt((2.0 * dl - 1.0) / (dl - dm) * (2.0 * dl + 1.0) / (dl + dm));
+}
+__device__ __forceinline__ double rec_b(int l, int m) {
+    double dl = l, dm = m;
+    return sqrt((dl + dm - 1.0) / (dl - dm) * (2.0 * dl + 1.0) / (2.0 * dl - 3.0) * (dl - dm - 1.0) / (dl + dm));
+}
+
+constexpr double kSeedLog2Floor = -600.0;
+
+// Start values of the recurrence for (m, north ring p); see file comment.
+// logc[m] = log2(Pbar_m^m / sin^m(theta)) = log2(1/sqrt(4pi)) + 0.5 sum_k log2((2k+1)/(2k)).
+__global__ void k_legendre_start(int M, int L, int nside, const RingPair* __restrict__ pairs,
+                                 const double* __restrict__ logc, int* __restrict__ lstart,
+                                 double2* __restrict__ pstart) {
+    const int NP = 2 * nside;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)M * NP) return;
+    const int m = (int)(idx / NP), p = (int)(idx % NP);
+    int ls = L;
+    double2 ps = make_double2(0.0, 0.0);
+    if (m < L && p >= first_ring_for_m(m, nside)) {
+        const double x = pairs[p].z;
+        const double s2 = ring_sin2(p, nside);
+        const double lg = logc[m] + 0.5 * (double)m * log2(s2);
+        // scaled pair: value = mant * 2^E
+        double E = floor(lg);
+        double q0 = exp2(lg - E);
+        double q1 = sqrt(2.0 * m + 3.0) * x * q0;
+        int l = m;
+        while (l < L) {
+            if (q0 != 0.0 && log2(fabs(q0)) + E >= kSeedLog2Floor) {
+                ls = l;
+                ps = make_double2(ldexp(q0, (int)E), ldexp(q1, (int)E));
+                break;
+            }
+            // advance one degree: q2 = a x q1 - b q0 at degree l+2
+            double q2 = rec_a(l + 2, m) * x * q1 - rec_b(l + 2, m) * q0;
+            q0 = q1;
+            q1 = q2;
+            ++l;
+            double mx = fmax(fabs(q0), fabs(q1));
+            if (mx > 0x1p500) {
+                q0 = ldexp(q0, -500);
+                q1 = ldexp(q1, -500);
+                E += 500.0;
+            }
+        }
+    }
+    lstart[idx] = ls;
+    pstart[idx] = ps;
+}
+
+// One FP64 recurrence step for degree l given (p1, p2) = (P_{l-1}, P_{l-2}).
+__device__ __forceinline__ double leg_step(int l, int ls, double2 ps, double a, double b, double x, double p1,
+                                           double p2) {
+    double v = a * x * p1 - b * p2;
+    v = (l == ls) ? ps.x : v;
+    v = (l == ls + 1) ? ps.y : v;
+    v = (l < ls) ? 0.0 : v;
+    return v;
+}
+
+// ------------------------------------------------------------ forward (analysis)
+// alm[b][l][m] = sum_{p >= t0(m)} Pbar_l^m(x_p) X[m][(l-m)&1][p][2b..2b+1]
+// One CTA per (m, column tile).  l-blocks of LT degrees; the FP64 recurrence
+// state of every ring lives in shared memory across l-blocks.  Column tile:
+// 128 columns = 64 maps (re/im interleaved).
+template <typename T>
+struct FwdCfg {
+    static constexpr int LT = 64;                       // degrees per l-block (32 even, 32 odd)
+    static constexpr int CT = 128;                      // columns per CTA
+    static constexpr int RB = sizeof(T) == 4 ? 256 : 128;  // rings generated per pass
+    static constexpr int KC = 16;                       // rings per staged X chunk
+    static constexpr int LTP = LT + 16 / sizeof(T);     // padded P row
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t fwd_smem_bytes(int L, int nside) {
+    using C = FwdCfg<T>;
+    return (size_t)2 * L * sizeof(double)                 // coefficients
+           + (size_t)2 * nside * (2 * sizeof(double) + sizeof(int))  // state + l_s
+           + (size_t)C::RB * C::LTP * sizeof(T)            // P tile
+           + (size_t)C::KC * 2 * C::CT * sizeof(T)         // X chunk
+           + 64;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec, int C, int nmaps,
+                                                      T* __restrict__ alm, int L, int M, int nside,
+                                                      const RingPair* __restrict__ pairs,
+                                                      const int* __restrict__ lstart,
+                                                      const double2* __restrict__ pstart, int accumulate) {
+    using Cfg = FwdCfg<T>;
+    constexpr int LT = Cfg::LT, CT = Cfg::CT, RB = Cfg::RB, KC = Cfg::KC, LTP = Cfg::LTP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NP = 2 * nside;
+    const int m = blockIdx.x;
+    const int c0 = blockIdx.y * CT;
+    const int tid = threadIdx.x;
+    double* coefA = (double*)smem_raw;
+    double* coefB = coefA + L;
+    double* st1 = coefB + L;
+    double* st2 = st1 + NP;
+    int* lsv = (int*)(st2 + NP);
+    T* Pt = (T*)(((uintptr_t)(lsv + NP) + 15) & ~(uintptr_t)15);
+    T* Xs = Pt + RB * LTP;
+
+    const int t0 = first_ring_for_m(m, nside);
+    const int K = m < L ? NP - t0 : 0;
+    const int lbeg = m < L ? m : L;
+
+    // zero the l < m triangle (and everything when no ring carries m)
+    if (!accumulate) {
+        const int nz = lbeg;
+        for (int i = tid; i < nz * (CT / 2); i += blockDim.x) {
+            int l = i / (CT / 2), j = i % (CT / 2);
+            int b = c0 / 2 + j;
+            if (b < nmaps) *(cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m)) = {(T)0, (T)0};
+        }
+    }
+    if (lbeg >= L) return;
+
+    for (int l = m + 2 + tid; l < L; l += blockDim.x) {
+        coefA[l] = rec_a(l, m);
+        coefB[l] = rec_b(l, m);
+    }
+    for (int r = tid; r < K; r += blockDim.x) {
+        st1[r] = 0.0;
+        st2[r] = 0.0;
+        lsv[r] = lstart[(int64_t)m * NP + t0 + r];
+    }
+    __syncthreads();
+
+    const int tx = tid & 15, ty = tid >> 4;
+    const int par = ty >> 3;           // 0: l-m even (S), 1: odd (D)
+    const int jrow = (ty & 7) * 4;     // 4 rows of this parity
+    const int cA = tx * 4, cB = 64 + tx * 4;
+
+    for (int l0 = m; l0 < L; l0 += LT) {
+        T acc[4][8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[i][c] = (T)0;
+
+        for (int rb = 0; rb < K; rb += RB) {
+            // --- generate Pbar for rings rb.., degrees l0..l0+LT
+            if (tid < RB) {
+                const int r = rb + tid;
+                T* prow = Pt + tid * LTP;
+                if (r < K) {
+                    const int p = t0 + r;
+                    const double x = pairs[p].z;
+                    double p1 = st1[r], p2 = st2[r];
+                    const int ls = lsv[r];
+                    double2 ps = make_double2(0.0, 0.0);
+                    if (ls + 1 >= l0 && ls < l0 + LT && ls < L) ps = pstart[(int64_t)m * NP + p];
+                    for (int i = 0; i < LT; ++i) {
+                        const int l = l0 + i;
+                        double v = 0.0;
+                        if (l < L) v = leg_step(l, ls, ps, l >= m + 2 ? coefA[l] : 0.0, l >= m + 2 ? coefB[l] : 0.0, x, p1, p2);
+                        p2 = p1;
+                        p1 = v;
+                        prow[(i & 1) * (LT / 2) + (i >> 1)] = (T)v;
+                    }
+                    st1[r] = p1;
+                    st2[r] = p2;
+                } else {
+                    for (int i = 0; i < LT; ++i) prow[i] = (T)0;
+                }
+            }
+            __syncthreads();
+            // --- contract against staged X chunks
+            const int rend = min(RB, K - rb);
+            for (int kc = 0; kc < rend; kc += KC) {
+                for (int i = tid; i < KC * 2 * CT; i += blockDim.x) {
+                    const int c = i % CT, q = (i / CT) >> 1, pr = (i / CT) & 1;
+                    const int r = rb + kc + q;
+                    T v = (T)0;
+                    if (r < K && c0 + c < C) v = spec[(((int64_t)m * 2 + pr) * NP + t0 + r) * C + c0 + c];
+                    Xs[(q * 2 + pr) * CT + c] = v;
+                }
+                __syncthreads();
+                const int qn = min(KC, rend - kc);
+                for (int q = 0; q < qn; ++q) {
+                    const T* pr = Pt + (kc + q) * LTP + par * (LT / 2) + jrow;
+                    T pv[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) pv[i] = pr[i];
+                    const T* xr = Xs + (q * 2 + par) * CT;
+                    T xv[8];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        xv[c] = xr[cA + c];
+                        xv[4 + c] = xr[cB + c];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) acc[i][c] = fma(pv[i], xv[c], acc[i][c]);
+                }
+                __syncthreads();
+            }
+        }
+        // --- write this l-block
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int l = l0 + 2 * (jrow + i) + par;
+            if (l >= L) continue;
+#pragma unroll
+            for (int cc = 0; cc < 8; cc += 2) {
+                const int c = c0 + (cc < 4 ? cA + cc : cB + cc - 4);
+                const int b = c >> 1;
+                if (b < nmaps) {
+                    cplx<T>* dst = (cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m));
+                    cplx<T> v = {acc[i][cc], acc[i][cc + 1]};
+                    if (accumulate) v = cadd(*dst, v);
+                    *dst = v;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ inverse (synthesis)
+// E[m][p][c] = sum_{l-m even} Pbar_l^m(x_p) A[m][l][c],  O = sum over l-m odd,
+// written to spec[m][0][p][c] and spec[m][1][p][c].  One CTA per (m, block of
+// RBI rings, column tile); the FP64 recurrence of each ring runs in one thread.
+template <typename T>
+struct InvCfg {
+    static constexpr int RBI = 64;  // rings per CTA
+    static constexpr int CT = 128;  // columns per CTA
+    static constexpr int LC = 32;   // degrees per staged chunk
+    static constexpr int RBP = RBI + 16 / sizeof(T);
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t inv_smem_bytes(int L) {
+    using C = InvCfg<T>;
+    return (size_t)2 * L * sizeof(double) + (size_t)C::LC * C::RBP * sizeof(T) + (size_t)C::LC * C::CT * sizeof(T) + 64;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT, int C, T* __restrict__ spec, int L,
+                                                      int M, int nside, const RingPair* __restrict__ pairs,
+                                                      const int* __restrict__ lstart,
+                                                      const double2* __restrict__ pstart,
+                                                      const int2* __restrict__ work) {
+    using Cfg = InvCfg<T>;
+    constexpr int RBI = Cfg::RBI, CT = Cfg::CT, LC = Cfg::LC, RBP = Cfg::RBP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NP = 2 * nside;
+    const int2 wk = work[blockIdx.x];
+    const int m = wk.x, rb = wk.y;
+    const int c0 = blockIdx.y * CT;
+    const int tid = threadIdx.x;
+    double* coefA = (double*)smem_raw;
+    double* coefB = coefA + L;
+    T* Pt = (T*)(((uintptr_t)(coefB + L) + 15) & ~(uintptr_t)15);  // [LC][RBP]
+    T* As = Pt + LC * RBP;                                          // [LC][CT]
+
+    const int t0 = first_ring_for_m(m, nside);
+    const int K = NP - t0;
+
+    for (int l = m + 2 + tid; l < L; l += blockDim.x) {
+        coefA[l] = rec_a(l, m);
+        coefB[l] = rec_b(l, m);
+    }
+    // generator state (threads tid < RBI own ring rb + tid)
+    const int rg = rb + tid;
+    const bool gen = tid < RBI && rg < K;
+    double x = 0.0, p1 = 0.0, p2 = 0.0;
+    int ls = L;
+    double2 ps = make_double2(0.0, 0.0);
+    if (gen) {
+        x = pairs[t0 + rg].z;
+        ls = lstart[(int64_t)m * NP + t0 + rg];
+        if (ls < L) ps = pstart[(int64_t)m * NP + t0 + rg];
+    }
+    __syncthreads();
+
+    const int tx = tid & 15, ty = tid >> 4;
+    const int rrow = ty * 4;
+    const int cA = tx * 4, cB = 64 + tx * 4;
+    T accE[4][8], accO[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            accE[i][c] = (T)0;
+            accO[i][c] = (T)0;
+        }
+
+    for (int l0 = m; l0 < L; l0 += LC) {
+        if (tid < RBI) {
+            for (int i = 0; i < LC; ++i) {
+                const int l = l0 + i;
+                double v = 0.0;
+                if (gen && l < L) v = leg_step(l, ls, ps, l >= m + 2 ? coefA[l] : 0.0, l >= m + 2 ? coefB[l] : 0.0, x, p1, p2);
+                p2 = p1;
+                p1 = v;
+                Pt[i * RBP + tid] = (T)v;
+            }
+        }
+        for (int i = tid; i < LC * CT; i += blockDim.x) {
+            const int c = i % CT, li = i / CT;
+            const int l = l0 + li;
+            T v = (T)0;
+            if (l < L && c0 + c < C) v = almT[((int64_t)m * L + l) * C + c0 + c];
+            As[li * CT + c] = v;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int li = 0; li < LC; li += 2) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const T* pr = Pt + (li + h) * RBP + rrow;
+                const T* ar = As + (li + h) * CT;
+                T pv[4], av[8];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) pv[i] = pr[i];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    av[c] = ar[cA + c];
+                    av[4 + c] = ar[cB + c];
+                }
+                if (h == 0) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) accE[i][c] = fma(pv[i], av[c], accE[i][c]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) accO[i][c] = fma(pv[i], av[c], accO[i][c]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // write E/O for rings of this CTA
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = rb + rrow + i;
+        if (r >= K) continue;
+        T* e = spec + (((int64_t)m * 2 + 0) * NP + t0 + r) * C + c0;
+        T* o = spec + (((int64_t)m * 2 + 1) * NP + t0 + r) * C + c0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int cc = c < 4 ? cA + c : cB + c - 4;
+            if (c0 + cc < C) {
+                e[cc] = accE[i][c];
+                o[cc] = accO[i][c];
+            }
+        }
+    }
+}
+
+}  // namespace hpx

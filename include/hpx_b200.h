@@ -1,0 +1,138 @@
+/*
+ * hpx_b200 -- HEALPix real spherical-harmonic transforms on NVIDIA B200 (sm_100a).
+ *
+ * C ABI of the transform library (libhpx_b200.so).  Every entry point returns
+ * an int status (hpx_status_t); no C++ exception crosses this boundary and the
+ * library never calls exit().  Pointers are plain device pointers; streams are
+ * cudaStream_t passed as void*.
+ *
+ * The functions replace the native layer of cuHPX's SHT path (paths relative
+ * to the cuHPX repository):
+ *   hpx_plan_create        cuhpx/hpx_sht.py:645-683, 696-730 (SHTCUDA/iSHTCUDA
+ *                          constructors: weights, Legendre table, W) and the
+ *                          HealpixFFT/HealpixIFFT plan singletons
+ *                          (src/harmonic_transform/hpx_fft.h:69-255)
+ *   hpx_sht_forward        cuhpx/hpx_sht.py:518-562 (SHTFunction.forward:
+ *                          healpix_rfft_batch, hpx_fft.cpp:21-84, + einsum)
+ *   hpx_sht_inverse        cuhpx/hpx_sht.py:589-611 (iSHTFunction.forward:
+ *                          einsum + healpix_irfft_batch, hpx_fft.cpp:86-149)
+ *   hpx_sht_forward_adjoint  exact adjoint of hpx_sht_forward; replaces the
+ *                          approximate SHTFunction.backward (hpx_sht.py:565-583)
+ *   hpx_sht_inverse_adjoint  exact adjoint of hpx_sht_inverse; replaces
+ *                          iSHTFunction.backward (hpx_sht.py:614-641)
+ *
+ * Data layouts (row-major, batch outermost):
+ *   map   [batch][12*nside^2]  real (float for FP32/mixed plans, double for FP64)
+ *   alm   [batch][lmax][mmax]  complex interleaved (re, im); entries m > l are 0
+ */
+#ifndef HPX_B200_H
+#define HPX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HPX_API __attribute__((visibility("default")))
+#else
+#define HPX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    HPX_OK = 0,
+    HPX_ERR_INVALID_ARG = 1,
+    HPX_ERR_OOM = 2,
+    HPX_ERR_CUDA = 3,
+    HPX_ERR_TIMEOUT = 4,
+    HPX_ERR_UNSUPPORTED = 5,
+    HPX_ERR_WORKSPACE = 6
+} hpx_status_t;
+
+/* Arithmetic of the Legendre contraction.  FFT stages run in float for
+ * FP32/BF16X3/TF32 plans and in double for FP64 plans. */
+typedef enum {
+    HPX_PREC_FP32 = 0,   /* FP32 SIMT contraction ("plain FP32 path") */
+    HPX_PREC_FP64 = 1,   /* FP64 everywhere (double I/O)              */
+    HPX_PREC_BF16X3 = 2, /* tcgen05 BF16 3-term split, FP32 accumulate */
+    HPX_PREC_TF32 = 3    /* tcgen05 TF32, FP32 accumulate             */
+} hpx_precision_t;
+
+typedef struct {
+    int32_t nside;               /* HEALPix resolution, >= 1                          */
+    int32_t lmax;                /* number of degrees l (l < lmax)                    */
+    int32_t mmax;                /* number of orders m (m < mmax)                     */
+    int32_t precision;           /* hpx_precision_t                                   */
+    int32_t refine_iters;        /* default Jacobi iterations of hpx_sht_forward_refined */
+    int32_t batch_chunk;         /* maps per internal pass (0 = default 64)           */
+    int32_t device;              /* CUDA device ordinal the plan lives on             */
+    int32_t flags;               /* reserved, must be 0                               */
+    const double* ring_weights;  /* host array of 2*nside FITS ring-weight corrections
+                                    (1 + w) factors are applied inside; NULL = uniform
+                                    4*pi/npix ("none" quadrature)                     */
+} hpx_desc_t;
+
+typedef struct hpx_plan_s* hpx_plan_t;
+
+/* Build a plan: ring tables, Legendre start values (FP64 on the GPU), Bluestein
+ * chirp spectra.  Immutable afterwards; usable concurrently from several streams
+ * provided each call gets its own workspace. */
+HPX_API int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan);
+HPX_API int hpx_plan_destroy(hpx_plan_t plan);
+
+/* Bytes of device workspace a call with `batch` maps needs (same for every op). */
+HPX_API int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes);
+
+/* Forward SHT (analysis): map -> alm. */
+HPX_API int hpx_sht_forward(hpx_plan_t plan, const void* map, void* alm, int64_t batch,
+                    void* workspace, size_t workspace_bytes, void* stream);
+/* Inverse SHT (synthesis): alm -> map.  Imag parts of m=0 (and of the ring
+ * Nyquist terms) are ignored, as an inverse real FFT does. */
+HPX_API int hpx_sht_inverse(hpx_plan_t plan, const void* alm, void* map, int64_t batch,
+                    void* workspace, size_t workspace_bytes, void* stream);
+/* Forward SHT followed by `iters` Jacobi refinement steps
+ *   alm <- alm + SHT(map - iSHT(alm))
+ * (iters < 0 uses the plan's refine_iters).  Each step costs one inverse and one
+ * forward transform; it removes the HEALPix quadrature error of band-limited
+ * maps and the rounding error of reduced-precision contractions. */
+HPX_API int hpx_sht_forward_refined(hpx_plan_t plan, const void* map, void* alm, int64_t batch, int32_t iters,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* Adjoint of hpx_sht_forward with respect to the real inner products
+ * <x,y> = sum x*y (maps) and Re sum conj(a)*b (alm): alm-gradient -> map-gradient. */
+HPX_API int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_grad, int64_t batch,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* Adjoint of hpx_sht_inverse: map-gradient -> alm-gradient. */
+HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Per-kernel timing.  While enabled, every kernel the plan launches is
+ * bracketed by CUDA events recorded on the launch stream; hpx_stats_read
+ * synchronises on those events and returns, per stage, the number of launches
+ * and their summed device time since the last read (then resets).  Leave it
+ * disabled while capturing a CUDA graph. */
+typedef struct {
+    const char* name;
+    int64_t launches;
+    double total_ms;
+} hpx_stage_stat_t;
+HPX_API int hpx_stats_enable(hpx_plan_t plan, int enable);
+HPX_API int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stages, int* n_stages);
+
+/* Plan geometry queries. */
+HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);
+
+/* Human-readable text of the last error seen by this plan (thread-local copy),
+ * and of a status code. */
+HPX_API const char* hpx_last_error(hpx_plan_t plan);
+HPX_API const char* hpx_status_string(int status);
+
+/* Library version string. */
+HPX_API const char* hpx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPX_B200_H */
