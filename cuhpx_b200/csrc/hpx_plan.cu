@@ -92,6 +92,10 @@ struct hpx_plan_s {
     double2* d_pstart = nullptr;
     int2* d_invwork = nullptr;
     int n_invwork = 0;
+    double2* d_coef = nullptr;   // [M][L] recurrence coefficients
+    double2* d_seeds = nullptr;  // [M][seed_blocks(L)][2*nside] block seeds
+    int2* d_fwdtiles = nullptr;  // (m, degree block) tiles of the forward contraction
+    int n_fwdtiles = 0;
     size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
@@ -128,6 +132,9 @@ struct hpx_plan_s {
         cudaFree(d_lstart);
         cudaFree(d_pstart);
         cudaFree(d_invwork);
+        cudaFree(d_coef);
+        cudaFree(d_seeds);
+        cudaFree(d_fwdtiles);
         tc_release(tc);
         for (auto& r : stats_recs) {
             cudaEventDestroy(r.a);
@@ -176,8 +183,10 @@ int create_typed(hpx_plan_s* P) {
         k_twiddles<double><<<(Pmax / 2 + 255) / 256, 256>>>(tw64, Pmax);
         HPX_CUDA_TRY(cudaMalloc(&P->d_gtab, (size_t)gsize * sizeof(C)));
         size_t sm = (size_t)Pmax * sizeof(cplx<double>);
-        if (sm > 48 * 1024)
-            HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int dmax = 0;
+        HPX_CUDA_TRY(cudaDeviceGetAttribute(&dmax, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
+        if ((int)sm > dmax) return set_err(HPX_ERR_UNSUPPORTED, "nside too large for the chirp precompute");
+        HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmax));
         k_chirp_spectra<T><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab);
         cudaError_t e = cudaGetLastError();
         cudaError_t e2 = cudaDeviceSynchronize();
@@ -187,16 +196,18 @@ int create_typed(hpx_plan_s* P) {
     }
     // shared memory budgets
     P->ring_smem = ring_smem_bytes<T>(P->bufP, P->mtmax, P->nmax);
-    P->fwd_smem = fwd_smem_bytes<T>(P->L, P->nside);
+    P->fwd_smem = fwd_smem_bytes<T>();
     P->inv_smem = inv_smem_bytes<T>(P->L);
     int dev_max = 0;
     HPX_CUDA_TRY(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
     if ((int)P->ring_smem > dev_max || (int)P->fwd_smem > dev_max || (int)P->inv_smem > dev_max)
         return set_err(HPX_ERR_UNSUPPORTED, "nside/lmax too large for the shared-memory kernels of this precision");
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->ring_smem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->ring_smem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->fwd_smem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P->inv_smem));
+    // The attribute is per function, not per plan: always raise it to the device
+    // maximum so that a plan needing less never lowers it under another plan.
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     return HPX_OK;
 }
 
@@ -278,6 +289,33 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     cudaFree(d_logc);
     if (e != cudaSuccess || e2 != cudaSuccess)
         return set_err(HPX_ERR_CUDA, std::string("legendre start: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+
+    // ---- recurrence coefficients and degree-block seeds (FP64)
+    HPX_CUDA_TRY(cudaMalloc(&P->d_coef, sizeof(double2) * (size_t)P->M * P->L));
+    {
+        const int64_t n = (int64_t)P->M * P->L;
+        k_legendre_coef<<<(unsigned)((n + 255) / 256), 256>>>(P->M, P->L, P->d_coef);
+        HPX_CUDA_TRY(cudaGetLastError());
+    }
+    const size_t nseed = (size_t)P->M * seed_blocks(P->L) * P->NP;
+    HPX_CUDA_TRY(cudaMalloc(&P->d_seeds, sizeof(double2) * nseed));
+    HPX_CUDA_TRY(cudaMemset(P->d_seeds, 0, sizeof(double2) * nseed));
+    k_legendre_seeds<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, N, P->d_pairs, P->d_lstart, P->d_pstart,
+                                                           P->d_coef, P->d_seeds);
+    e = cudaGetLastError();
+    e2 = cudaDeviceSynchronize();
+    if (e != cudaSuccess || e2 != cudaSuccess)
+        return set_err(HPX_ERR_CUDA, std::string("legendre seeds: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    {
+        std::vector<int2> tiles;
+        for (int m = 0; m < P->M; ++m) {
+            const int nb = m < P->L ? (P->L - m + kSeedBlock - 1) / kSeedBlock : 1;
+            for (int j = 0; j < nb; ++j) tiles.push_back(make_int2(m, j));
+        }
+        P->n_fwdtiles = (int)tiles.size();
+        HPX_CUDA_TRY(cudaMalloc(&P->d_fwdtiles, sizeof(int2) * tiles.size()));
+        HPX_CUDA_TRY(cudaMemcpy(P->d_fwdtiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+    }
 
     // ---- inverse work list: (m, ring block), heaviest first
     std::vector<int2> work;
@@ -380,9 +418,10 @@ struct Pipeline {
                        P->d_pstart, accumulate, st);
             return;
         }
-        dim3 grid(P->M, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
+        dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
         k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->nside, P->d_pairs,
-                                                          P->d_lstart, P->d_pstart, accumulate);
+                                                          P->d_lstart, P->d_pstart, P->d_coef, P->d_seeds,
+                                                          P->d_fwdtiles, accumulate);
     }
     void leg_inv(const T* alm, int nb) {
         const int C = P->cols();
@@ -400,7 +439,7 @@ struct Pipeline {
         if (P->n_invwork == 0) return;
         dim3 grid(P->n_invwork, (C + InvCfg<T>::CT - 1) / InvCfg<T>::CT);
         k_leg_inv_simt<T><<<grid, 256, P->inv_smem, st>>>(almT, C, spec, P->L, P->M, P->nside, P->d_pairs,
-                                                          P->d_lstart, P->d_pstart, P->d_invwork);
+                                                          P->d_lstart, P->d_pstart, P->d_coef, P->d_invwork);
     }
 };
 

@@ -90,14 +90,58 @@ __device__ __forceinline__ double leg_step(int l, int ls, double2 ps, double a, 
     return v;
 }
 
+// Recurrence coefficients a_lm, b_lm for every (m, l >= m+2), shared by the
+// seed precompute and all contraction kernels: coef[m * L + l] = (a, b).
+__global__ void k_legendre_coef(int M, int L, double2* __restrict__ coef) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)M * L) return;
+    const int m = (int)(idx / L), l = (int)(idx % L);
+    coef[idx] = l >= m + 2 ? make_double2(rec_a(l, m), rec_b(l, m)) : make_double2(0.0, 0.0);
+}
+
+// Degree-block seeds: for every (m, block j, north ring p) the FP64 pair
+// (Pbar_{l0}, Pbar_{l0+1}) at l0 = m + j*kSeedBlock, so that any block of
+// degrees can be generated independently.  Thread per (m, ring).
+constexpr int kSeedBlock = 64;
+
+__host__ __device__ inline int seed_blocks(int L) { return (L + kSeedBlock - 1) / kSeedBlock; }
+
+__global__ void k_legendre_seeds(int M, int L, int nside, const RingPair* __restrict__ pairs,
+                                 const int* __restrict__ lstart, const double2* __restrict__ pstart,
+                                 const double2* __restrict__ coef, double2* __restrict__ seeds) {
+    const int NP = 2 * nside;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)M * NP) return;
+    const int m = (int)(idx / NP), p = (int)(idx % NP);
+    const int nb = seed_blocks(L);
+    double2* out = seeds + (int64_t)m * nb * NP + p;
+    if (m >= L) return;
+    const int ls = lstart[idx];
+    const double2 ps = pstart[idx];
+    const double x = pairs[p].z;
+    double p1 = 0.0, p2 = 0.0;
+    const double2* cm = coef + (int64_t)m * L;
+    for (int l = m; l < L; ++l) {
+        double2 ab = l >= m + 2 ? cm[l] : make_double2(0.0, 0.0);
+        double v = leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2);
+        const int off = (l - m) % kSeedBlock;
+        const int j = (l - m) / kSeedBlock;
+        if (off == 0) out[(int64_t)j * NP] = make_double2(v, 0.0);
+        else if (off == 1) out[(int64_t)j * NP].y = v;
+        p2 = p1;
+        p1 = v;
+    }
+}
+
 // ------------------------------------------------------------ forward (analysis)
 // alm[b][l][m] = sum_{p >= t0(m)} Pbar_l^m(x_p) X[m][(l-m)&1][p][2b..2b+1]
-// One CTA per (m, column tile).  l-blocks of LT degrees; the FP64 recurrence
-// state of every ring lives in shared memory across l-blocks.  Column tile:
-// 128 columns = 64 maps (re/im interleaved).
+// One CTA per (m, degree block of 64, column tile of 128 = 64 maps).  Each
+// pass generates Pbar for RB rings x 64 degrees from the FP64 block seeds
+// (one ring per thread), then contracts it with X chunks that cp.async
+// double-buffers through shared memory.
 template <typename T>
 struct FwdCfg {
-    static constexpr int LT = 64;                       // degrees per l-block (32 even, 32 odd)
+    static constexpr int LT = kSeedBlock;               // degrees per tile (32 even, 32 odd)
     static constexpr int CT = 128;                      // columns per CTA
     static constexpr int RB = sizeof(T) == 4 ? 256 : 128;  // rings generated per pass
     static constexpr int KC = 16;                       // rings per staged X chunk
@@ -105,148 +149,177 @@ struct FwdCfg {
 };
 
 template <typename T>
-__host__ __device__ constexpr size_t fwd_smem_bytes(int L, int nside) {
+__host__ __device__ constexpr size_t fwd_smem_bytes() {
     using C = FwdCfg<T>;
-    return (size_t)2 * L * sizeof(double)                 // coefficients
-           + (size_t)2 * nside * (2 * sizeof(double) + sizeof(int))  // state + l_s
-           + (size_t)C::RB * C::LTP * sizeof(T)            // P tile
-           + (size_t)C::KC * 2 * C::CT * sizeof(T)         // X chunk
-           + 64;
+    return (size_t)C::LT * sizeof(double2) + (size_t)C::RB * C::LTP * sizeof(T) +
+           (size_t)2 * C::KC * 2 * C::CT * sizeof(T) + 64;
 }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec, int C, int nmaps,
                                                       T* __restrict__ alm, int L, int M, int nside,
                                                       const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
-                                                      const double2* __restrict__ pstart, int accumulate) {
+                                                      const double2* __restrict__ pstart,
+                                                      const double2* __restrict__ coef,
+                                                      const double2* __restrict__ seeds,
+                                                      const int2* __restrict__ tiles, int accumulate) {
     using Cfg = FwdCfg<T>;
     constexpr int LT = Cfg::LT, CT = Cfg::CT, RB = Cfg::RB, KC = Cfg::KC, LTP = Cfg::LTP;
+    constexpr int VPR = CT * sizeof(T) / 16;  // 16-byte vectors per staged row
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = 2 * nside;
-    const int m = blockIdx.x;
+    const int2 tl = tiles[blockIdx.x];
+    const int m = tl.x, jb = tl.y;
+    const int l0 = m + jb * LT;
     const int c0 = blockIdx.y * CT;
     const int tid = threadIdx.x;
-    double* coefA = (double*)smem_raw;
-    double* coefB = coefA + L;
-    double* st1 = coefB + L;
-    double* st2 = st1 + NP;
-    int* lsv = (int*)(st2 + NP);
-    T* Pt = (T*)(((uintptr_t)(lsv + NP) + 15) & ~(uintptr_t)15);
-    T* Xs = Pt + RB * LTP;
+    double2* cf = (double2*)smem_raw;
+    T* Pt = (T*)(cf + LT);
+    T* Xs = Pt + RB * LTP;  // [2][KC][2][CT]
 
     const int t0 = first_ring_for_m(m, nside);
-    const int K = m < L ? NP - t0 : 0;
-    const int lbeg = m < L ? m : L;
+    const int K = NP - t0;
+    const int nbk = seed_blocks(L);
 
-    // zero the l < m triangle (and everything when no ring carries m)
-    if (!accumulate) {
-        const int nz = lbeg;
-        for (int i = tid; i < nz * (CT / 2); i += blockDim.x) {
-            int l = i / (CT / 2), j = i % (CT / 2);
-            int b = c0 / 2 + j;
+    // zero the l < m triangle once per (m, column tile)
+    if (!accumulate && jb == 0) {
+        for (int i = tid; i < min(m, L) * (CT / 2); i += blockDim.x) {
+            const int l = i / (CT / 2), b = c0 / 2 + i % (CT / 2);
             if (b < nmaps) *(cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m)) = {(T)0, (T)0};
         }
     }
-    if (lbeg >= L) return;
-
-    for (int l = m + 2 + tid; l < L; l += blockDim.x) {
-        coefA[l] = rec_a(l, m);
-        coefB[l] = rec_b(l, m);
+    if (m >= L) return;
+    for (int i = tid; i < LT; i += blockDim.x) {
+        const int l = l0 + i;
+        cf[i] = (l < L && l >= m + 2) ? coef[(int64_t)m * L + l] : make_double2(0.0, 0.0);
     }
-    for (int r = tid; r < K; r += blockDim.x) {
-        st1[r] = 0.0;
-        st2[r] = 0.0;
-        lsv[r] = lstart[(int64_t)m * NP + t0 + r];
-    }
-    __syncthreads();
 
     const int tx = tid & 15, ty = tid >> 4;
-    const int par = ty >> 3;           // 0: l-m even (S), 1: odd (D)
-    const int jrow = (ty & 7) * 4;     // 4 rows of this parity
+    const int par = ty >> 3;        // 0: l-m even (S), 1: odd (D)
+    const int jrow = (ty & 7) * 4;  // 4 rows of this parity
     const int cA = tx * 4, cB = 64 + tx * 4;
-
-    for (int l0 = m; l0 < L; l0 += LT) {
-        T acc[4][8];
+    T acc[4][8];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) acc[i][c] = (T)0;
+        for (int c = 0; c < 8; ++c) acc[i][c] = (T)0;
 
-        for (int rb = 0; rb < K; rb += RB) {
-            // --- generate Pbar for rings rb.., degrees l0..l0+LT
-            if (tid < RB) {
-                const int r = rb + tid;
-                T* prow = Pt + tid * LTP;
-                if (r < K) {
-                    const int p = t0 + r;
-                    const double x = pairs[p].z;
-                    double p1 = st1[r], p2 = st2[r];
-                    const int ls = lsv[r];
-                    double2 ps = make_double2(0.0, 0.0);
-                    if (ls + 1 >= l0 && ls < l0 + LT && ls < L) ps = pstart[(int64_t)m * NP + p];
-                    for (int i = 0; i < LT; ++i) {
-                        const int l = l0 + i;
-                        double v = 0.0;
-                        if (l < L) v = leg_step(l, ls, ps, l >= m + 2 ? coefA[l] : 0.0, l >= m + 2 ? coefB[l] : 0.0, x, p1, p2);
+    auto stage = [&](int buf, int rbase, int nr) {
+        T* dst = Xs + buf * (KC * 2 * CT);
+        for (int i = tid; i < KC * 2 * VPR; i += blockDim.x) {
+            const int v = i % VPR, row = i / VPR;
+            const int q = row >> 1, pr = row & 1;
+            const int r = rbase + q;
+            const int c = c0 + v * (16 / (int)sizeof(T));
+            const bool ok = q < nr && c < C;
+            const T* src = spec + (((int64_t)m * 2 + pr) * NP + t0 + (ok ? r : 0)) * C + (ok ? c : 0);
+            cp_async16(dst + row * CT + v * (16 / sizeof(T)), src, ok);
+        }
+        cp_async_commit();
+    };
+
+    for (int rb = 0; rb < K; rb += RB) {
+        __syncthreads();  // coefficient table ready / previous pass done with Pt
+        // --- generate Pbar for rings rb.., degrees l0..l0+LT from the block seeds
+        if (tid < RB) {
+            const int r = rb + tid;
+            T* prow = Pt + tid * LTP;
+            if (r < K) {
+                const int p = t0 + r;
+                const int64_t mi = (int64_t)m * NP + p;
+                const double x = pairs[p].z;
+                const int ls = lstart[mi];
+                const double2 sd = seeds[((int64_t)m * nbk + jb) * NP + p];
+                double p2 = 0.0, p1 = 0.0;
+                if (ls <= l0) {
+                    // fast path: the seed pair is exact
+                    prow[0] = (T)sd.x;
+                    if (LT > 1) prow[LT / 2] = (T)sd.y;
+                    p2 = sd.x;
+                    p1 = sd.y;
+#pragma unroll 4
+                    for (int i = 2; i < LT; ++i) {
+                        const double2 ab = cf[i];
+                        const double v = (l0 + i < L) ? ab.x * x * p1 - ab.y * p2 : 0.0;
                         p2 = p1;
                         p1 = v;
                         prow[(i & 1) * (LT / 2) + (i >> 1)] = (T)v;
                     }
-                    st1[r] = p1;
-                    st2[r] = p2;
                 } else {
-                    for (int i = 0; i < LT; ++i) prow[i] = (T)0;
-                }
-            }
-            __syncthreads();
-            // --- contract against staged X chunks
-            const int rend = min(RB, K - rb);
-            for (int kc = 0; kc < rend; kc += KC) {
-                for (int i = tid; i < KC * 2 * CT; i += blockDim.x) {
-                    const int c = i % CT, q = (i / CT) >> 1, pr = (i / CT) & 1;
-                    const int r = rb + kc + q;
-                    T v = (T)0;
-                    if (r < K && c0 + c < C) v = spec[(((int64_t)m * 2 + pr) * NP + t0 + r) * C + c0 + c];
-                    Xs[(q * 2 + pr) * CT + c] = v;
-                }
-                __syncthreads();
-                const int qn = min(KC, rend - kc);
-                for (int q = 0; q < qn; ++q) {
-                    const T* pr = Pt + (kc + q) * LTP + par * (LT / 2) + jrow;
-                    T pv[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) pv[i] = pr[i];
-                    const T* xr = Xs + (q * 2 + par) * CT;
-                    T xv[8];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        xv[c] = xr[cA + c];
-                        xv[4 + c] = xr[cB + c];
+                    const double2 ps = (ls < l0 + LT && ls < L) ? pstart[mi] : make_double2(0.0, 0.0);
+                    for (int i = 0; i < LT; ++i) {
+                        const int l = l0 + i;
+                        const double2 ab = cf[i];
+                        const double v = (l < L) ? leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2) : 0.0;
+                        p2 = p1;
+                        p1 = v;
+                        prow[(i & 1) * (LT / 2) + (i >> 1)] = (T)v;
                     }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) acc[i][c] = fma(pv[i], xv[c], acc[i][c]);
                 }
-                __syncthreads();
+            } else {
+                for (int i = 0; i < LT; ++i) prow[i] = (T)0;
             }
         }
-        // --- write this l-block
+        const int rend = min(RB, K - rb);
+        const int nch = (rend + KC - 1) / KC;
+        stage(0, rb, min(KC, rend));
+        __syncthreads();
+        for (int ch = 0; ch < nch; ++ch) {
+            if (ch + 1 < nch) {
+                stage((ch + 1) & 1, rb + (ch + 1) * KC, min(KC, rend - (ch + 1) * KC));
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            const T* xb = Xs + (ch & 1) * (KC * 2 * CT);
+            const int qn = min(KC, rend - ch * KC);
+            const T* pbase = Pt + (ch * KC) * LTP + par * (LT / 2) + jrow;
+#pragma unroll 4
+            for (int q = 0; q < qn; ++q) {
+                const T* pr = pbase + q * LTP;
+                T pv[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int l = l0 + 2 * (jrow + i) + par;
-            if (l >= L) continue;
+                for (int i = 0; i < 4; ++i) pv[i] = pr[i];
+                const T* xr = xb + (q * 2 + par) * CT;
+                T xv[8];
 #pragma unroll
-            for (int cc = 0; cc < 8; cc += 2) {
-                const int c = c0 + (cc < 4 ? cA + cc : cB + cc - 4);
-                const int b = c >> 1;
-                if (b < nmaps) {
-                    cplx<T>* dst = (cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m));
-                    cplx<T> v = {acc[i][cc], acc[i][cc + 1]};
-                    if (accumulate) v = cadd(*dst, v);
-                    *dst = v;
+                for (int c = 0; c < 4; ++c) {
+                    xv[c] = xr[cA + c];
+                    xv[4 + c] = xr[cB + c];
                 }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) acc[i][c] = fma(pv[i], xv[c], acc[i][c]);
+            }
+            __syncthreads();
+        }
+    }
+    // --- write this tile
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int l = l0 + 2 * (jrow + i) + par;
+        if (l >= L) continue;
+#pragma unroll
+        for (int cc = 0; cc < 8; cc += 2) {
+            const int c = c0 + (cc < 4 ? cA + cc : cB + cc - 4);
+            const int b = c >> 1;
+            if (b < nmaps) {
+                cplx<T>* dst = (cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m));
+                cplx<T> v = {acc[i][cc], acc[i][cc + 1]};
+                if (accumulate) v = cadd(*dst, v);
+                *dst = v;
             }
         }
     }
@@ -275,6 +348,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
                                                       int M, int nside, const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
                                                       const double2* __restrict__ pstart,
+                                                      const double2* __restrict__ coef,
                                                       const int2* __restrict__ work) {
     using Cfg = InvCfg<T>;
     constexpr int RBI = Cfg::RBI, CT = Cfg::CT, LC = Cfg::LC, RBP = Cfg::RBP;
@@ -293,8 +367,9 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
     const int K = NP - t0;
 
     for (int l = m + 2 + tid; l < L; l += blockDim.x) {
-        coefA[l] = rec_a(l, m);
-        coefB[l] = rec_b(l, m);
+        const double2 ab = coef[(int64_t)m * L + l];
+        coefA[l] = ab.x;
+        coefB[l] = ab.y;
     }
     // generator state (threads tid < RBI own ring rb + tid)
     const int rg = rb + tid;
