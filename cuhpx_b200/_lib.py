@@ -50,6 +50,7 @@ class HpxStageStat(ctypes.Structure):
 
 SIGNATURES = {
     "hpx_stats_enable": ([_vp, ctypes.c_int], ctypes.c_int),
+    "hpx_plan_check": ([_vp, _vp], ctypes.c_int),
     "hpx_stats_read": ([_vp, ctypes.POINTER(HpxStageStat), ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "hpx_plan_create": ([ctypes.POINTER(HpxDesc), ctypes.POINTER(_vp)], ctypes.c_int),
     "hpx_plan_destroy": ([_vp], ctypes.c_int),

@@ -62,7 +62,6 @@ def build(force=False, debug=False, verbose=False):
         "-o",
         LIB + ".tmp",
         *[os.path.join(CSRC, s) for s in SOURCES],
-        "-lcuda",
     ]
     if debug:
         cmd.insert(1, "-DHPX_CHECK_BOUNDS=1")

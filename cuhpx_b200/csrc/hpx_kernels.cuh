@@ -2,6 +2,7 @@
 #pragma once
 
 #include "legendre.cuh"
+#include "tc_ptx.cuh"
 
 namespace hpx {
 
@@ -19,11 +20,14 @@ __host__ __device__ constexpr size_t ring_smem_bytes(int bufP, int mtmax, int nm
 }
 
 // map[b][npix] -> spec[m][0|1][p][c]
+// With xh != nullptr (mixed-precision plans) the folded spectra are written as
+// bf16 hi/lo pairs xh/xl[m][par][p][c] instead of T values in spec.
 template <typename T>
 __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
                                                   T* __restrict__ spec, int C, int nside, int mtmax, int bufP,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
-                                                  int logPmax, const cplx<T>* __restrict__ gtab, int mode) {
+                                                  int logPmax, const cplx<T>* __restrict__ gtab, int mode,
+                                                  uint32_t* __restrict__ xh, uint32_t* __restrict__ xl) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = 2 * nside;
     const int p = blockIdx.x;
@@ -59,8 +63,22 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
                 S = cscale(Fn[k], wk);
                 D = {(T)0, (T)0};
             }
-            *(cplx<T>*)(spec + (((int64_t)k * 2 + 0) * NP + p) * C + 2 * b) = S;
-            *(cplx<T>*)(spec + (((int64_t)k * 2 + 1) * NP + p) * C + 2 * b) = D;
+            const int64_t i0 = (((int64_t)k * 2 + 0) * NP + p) * C + 2 * b;
+            const int64_t i1 = (((int64_t)k * 2 + 1) * NP + p) * C + 2 * b;
+            if (xh) {
+                uint16_t h0, l0, h1, l1;
+                tc::split_bf16((float)S.re, h0, l0);
+                tc::split_bf16((float)S.im, h1, l1);
+                xh[i0 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+                xl[i0 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+                tc::split_bf16((float)D.re, h0, l0);
+                tc::split_bf16((float)D.im, h1, l1);
+                xh[i1 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+                xl[i1 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+            } else {
+                *(cplx<T>*)(spec + i0) = S;
+                *(cplx<T>*)(spec + i1) = D;
+            }
         }
         __syncthreads();
     }

@@ -20,6 +20,7 @@
 //     with c_m = 2 for 0 < m < nphi/2 and 1 for m = 0, nphi/2.
 // The reference's hand-written backward (cuhpx/hpx_sht.py:565-583, 614-641)
 // halves the m = 0 term and mishandles the ring Nyquist terms; these do not.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -92,7 +93,8 @@ struct hpx_plan_s {
     double2* d_pstart = nullptr;
     int2* d_invwork = nullptr;
     int n_invwork = 0;
-    double2* d_coef = nullptr;   // [M][L] recurrence coefficients
+    int Lpad = 0;                // coefficient row length (L + kCoefPad)
+    double2* d_coef = nullptr;   // [M][Lpad] recurrence coefficients
     double2* d_seeds = nullptr;  // [M][seed_blocks(L)][2*nside] block seeds
     int2* d_fwdtiles = nullptr;  // (m, degree block) tiles of the forward contraction
     int n_fwdtiles = 0;
@@ -135,7 +137,9 @@ struct hpx_plan_s {
         cudaFree(d_coef);
         cudaFree(d_seeds);
         cudaFree(d_fwdtiles);
-        tc_release(tc);
+        cudaFree(tc.d_err);
+        cudaFree(tc.d_fwd_tiles);
+        cudaFree(tc.d_inv_tiles);
         for (auto& r : stats_recs) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
@@ -149,6 +153,9 @@ struct hpx_plan_s {
     size_t spec_bytes() const { return (size_t)M * 2 * NP * cols() * real_size(); }
     size_t almT_bytes() const { return (size_t)M * L * cols() * real_size(); }
     size_t resid_bytes() const { return (size_t)batch_chunk * npix * real_size(); }
+    bool mixed() const { return prec == HPX_PREC_BF16X3; }
+    // bf16 hi/lo synthesis operand [2M][Lh][128] x 2
+    size_t tcA_bytes() const { return mixed() ? (size_t)2 * 2 * M * tc.Lh * kTcCols * sizeof(uint16_t) : 0; }
 };
 
 namespace {
@@ -209,6 +216,71 @@ int create_typed(hpx_plan_s* P) {
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     return HPX_OK;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Tensor-core plan: tile lists, error flag, tensor-map encoder.
+int tc_create(hpx_plan_s* P) {
+    TcPlan& T = P->tc;
+    if (P->batch_chunk != 64)
+        return set_err(HPX_ERR_UNSUPPORTED, "bf16x3 plans process 64 maps per pass (batch_chunk must be 64)");
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    HPX_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) return set_err(HPX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+    T.encode = fn;
+    HPX_CUDA_TRY(cudaDeviceGetAttribute(&T.nsm, cudaDevAttrMultiProcessorCount, P->device));
+    HPX_CUDA_TRY(cudaMalloc(&T.d_err, sizeof(int)));
+    HPX_CUDA_TRY(cudaMemset(T.d_err, 0, sizeof(int)));
+    const int N = P->nside;
+    T.m_tc_end = std::min(std::min(P->L, P->M), 2 * N + 1);
+    T.Lh = (P->L + 65) / 2;
+    std::vector<int2> ft, it;
+    for (int m = 0; m < T.m_tc_end; ++m) {
+        for (int j = 0; j < (P->L - m + kTcFwdDeg - 1) / kTcFwdDeg; ++j) ft.push_back(make_int2(m, j));
+        const int K = P->NP - first_ring_for_m(m, N);
+        for (int rb = 0; rb < K; rb += kTcInvRings) it.push_back(make_int2(m, rb));
+    }
+    T.n_fwd_tiles = (int)ft.size();
+    T.n_inv_tiles = (int)it.size();
+    if (!ft.empty()) {
+        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_tiles, sizeof(int2) * ft.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_tiles, ft.data(), sizeof(int2) * ft.size(), cudaMemcpyHostToDevice));
+    }
+    if (!it.empty()) {
+        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * it.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
+    }
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    T.active = 1;
+    return HPX_OK;
+}
+
+// 3-D bf16 tensor map over [outer][rows][128 cols] with a {64 cols, 32 rows} box, 128B swizzle.
+int encode_operand(const hpx_plan_s* P, CUtensorMap* map, void* base, uint64_t rows, uint64_t outer) {
+    const cuuint64_t dims[3] = {(cuuint64_t)kTcCols, rows, outer};
+    const cuuint64_t strides[2] = {(cuuint64_t)kTcCols * 2, (cuuint64_t)kTcCols * 2 * rows};
+    const cuuint32_t box[3] = {64, 32, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = ((EncodeTiledFn)P->tc.encode)(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, es,
+                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(HPX_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return HPX_OK;
+}
+
+// zero alm[b][*][m] for m in [m0, M)
+__global__ void k_zero_alm_cols(float* __restrict__ alm, int nmaps, int L, int M, int m0) {
+    const int64_t n = (int64_t)nmaps * L * (M - m0);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int m = m0 + (int)(i % (M - m0));
+        const int64_t bl = i / (M - m0);
+        *(float2*)(alm + 2 * (bl * M + m)) = make_float2(0.f, 0.f);
+    }
 }
 
 int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
@@ -291,17 +363,18 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
         return set_err(HPX_ERR_CUDA, std::string("legendre start: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
 
     // ---- recurrence coefficients and degree-block seeds (FP64)
-    HPX_CUDA_TRY(cudaMalloc(&P->d_coef, sizeof(double2) * (size_t)P->M * P->L));
+    P->Lpad = P->L + kCoefPad;
+    HPX_CUDA_TRY(cudaMalloc(&P->d_coef, sizeof(double2) * (size_t)P->M * P->Lpad));
     {
-        const int64_t n = (int64_t)P->M * P->L;
-        k_legendre_coef<<<(unsigned)((n + 255) / 256), 256>>>(P->M, P->L, P->d_coef);
+        const int64_t n = (int64_t)P->M * P->Lpad;
+        k_legendre_coef<<<(unsigned)((n + 255) / 256), 256>>>(P->M, P->L, P->Lpad, P->d_coef);
         HPX_CUDA_TRY(cudaGetLastError());
     }
     const size_t nseed = (size_t)P->M * seed_blocks(P->L) * P->NP;
     HPX_CUDA_TRY(cudaMalloc(&P->d_seeds, sizeof(double2) * nseed));
     HPX_CUDA_TRY(cudaMemset(P->d_seeds, 0, sizeof(double2) * nseed));
-    k_legendre_seeds<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, N, P->d_pairs, P->d_lstart, P->d_pstart,
-                                                           P->d_coef, P->d_seeds);
+    k_legendre_seeds<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, P->Lpad, N, P->d_pairs, P->d_lstart,
+                                                           P->d_pstart, P->d_coef, P->d_seeds);
     e = cudaGetLastError();
     e2 = cudaDeviceSynchronize();
     if (e != cudaSuccess || e2 != cudaSuccess)
@@ -333,9 +406,10 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
 
     int rc = P->f64 ? create_typed<double>(P) : create_typed<float>(P);
     if (rc != HPX_OK) return rc;
-    if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
-        rc = tc_create(P->tc, P->prec, P->nside, P->L, P->M, P->batch_chunk, P->device);
-        if (rc != HPX_OK) return set_err(rc, std::string("tensor-core plan: ") + tc_last_error());
+    if (P->prec == HPX_PREC_TF32) return set_err(HPX_ERR_UNSUPPORTED, "tf32 contraction is not built; use bf16x3");
+    if (P->mixed()) {
+        rc = tc_create(P);
+        if (rc != HPX_OK) return rc;
     }
     return HPX_OK;
 }
@@ -361,6 +435,8 @@ struct Pipeline {
     T* spec;
     T* almT;
     T* resid;
+    uint16_t* tcA;  // bf16 hi/lo synthesis operand (mixed plans)
+    int rc = HPX_OK;
 
     Pipeline(const hpx_plan_s* p, void* ws, cudaStream_t s) : P(p), st(s) {
         char* c = (char*)ws;
@@ -369,6 +445,13 @@ struct Pipeline {
         almT = (T*)c;
         c += (P->almT_bytes() + 255) & ~(size_t)255;
         resid = (T*)c;
+        c += (P->resid_bytes() + 255) & ~(size_t)255;
+        tcA = (uint16_t*)c;
+    }
+    // folded spectra as bf16 hi/lo (mixed plans), aliasing the spec region
+    uint32_t* xh() const { return P->mixed() ? (uint32_t*)spec : nullptr; }
+    uint32_t* xl() const {
+        return P->mixed() ? (uint32_t*)((uint16_t*)spec + (size_t)2 * P->M * P->NP * kTcCols) : nullptr;
     }
 
     int maps_per_cta(int nb) const { return std::min(nb, 4); }
@@ -400,7 +483,7 @@ struct Pipeline {
         Timer tm(P, st, kStRingFwd);
         k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, spec, P->cols(), P->nside, P->mtmax, P->bufP,
                                                       P->d_pairs, (const cplx<T>*)P->d_tw, P->logPmax,
-                                                      (const cplx<T>*)P->d_gtab, mode);
+                                                      (const cplx<T>*)P->d_gtab, mode, xh(), xl());
     }
     void ring_inv(T* map, int nb, int mode, const T* ref) {
         const int g = maps_per_cta(nb);
@@ -413,33 +496,60 @@ struct Pipeline {
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();
         Timer tm(P, st, kStLegFwd);
-        if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
-            tc_forward(P->tc, (const float*)spec, C, nb, (float*)alm, P->L, P->M, P->nside, P->d_pairs, P->d_lstart,
-                       P->d_pstart, accumulate, st);
+        if (P->mixed()) {
+            const TcPlan& TP = P->tc;
+            if (!accumulate && TP.m_tc_end < P->M)
+                k_zero_alm_cols<<<1024, 256, 0, st>>>((float*)alm, nb, P->L, P->M, TP.m_tc_end);
+            if (TP.n_fwd_tiles == 0) return;
+            CUtensorMap mh, ml;
+            if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M)) != HPX_OK) return;
+            if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M)) != HPX_OK) return;
+            k_leg_fwd_tc<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kTcSmem, st>>>(
+                mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_pairs, P->d_lstart, P->d_pstart,
+                P->d_coef, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, TP.d_err);
             return;
         }
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
         k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->nside, P->d_pairs,
-                                                          P->d_lstart, P->d_pstart, P->d_coef, P->d_seeds,
+                                                          P->d_lstart, P->d_pstart, P->d_coef, P->Lpad, P->d_seeds,
                                                           P->d_fwdtiles, accumulate);
     }
     void leg_inv(const T* alm, int nb) {
         const int C = P->cols();
+        if (P->mixed()) {
+            const TcPlan& TP = P->tc;
+            uint16_t* ah = tcA;
+            uint16_t* al = tcA + (size_t)2 * P->M * TP.Lh * kTcCols;
+            {
+                Timer tm(P, st, kStAlmCols);
+                dim3 tg((P->M + 31) / 32, P->L + 64);
+                k_alm_to_tc<<<tg, dim3(32, 8), 0, st>>>((const float*)alm, nb, P->L, P->M, TP.Lh, ah, al);
+            }
+            Timer tm(P, st, kStLegInv);
+            // orders the tensor cores do not visit must read as zero in the ring stage
+            if (TP.m_tc_end < P->M)
+                cudaMemsetAsync(spec + (size_t)TP.m_tc_end * 2 * P->NP * C, 0,
+                                (size_t)(P->M - TP.m_tc_end) * 2 * P->NP * C * sizeof(T), st);
+            if (TP.n_inv_tiles == 0) return;
+            CUtensorMap mh, ml;
+            if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M)) != HPX_OK) return;
+            if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M)) != HPX_OK) return;
+            k_leg_inv_tc<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kTcSmem, st>>>(
+                mh, ml, (float*)spec, C, P->L, P->M, P->Lpad, P->nside, P->d_pairs, P->d_lstart, P->d_pstart,
+                P->d_coef, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, TP.d_err);
+            return;
+        }
         dim3 tg((P->M + 31) / 32, P->L, (nb + 15) / 16);
         {
             Timer tm(P, st, kStAlmCols);
             k_alm_to_cols<T><<<tg, dim3(32, 8), 0, st>>>(alm, nb, P->L, P->M, almT, C);
         }
         Timer tm(P, st, kStLegInv);
-        if (P->prec == HPX_PREC_BF16X3 || P->prec == HPX_PREC_TF32) {
-            tc_inverse(P->tc, (const float*)almT, C, (float*)spec, P->L, P->M, P->nside, P->d_pairs, P->d_lstart,
-                       P->d_pstart, P->d_invwork, P->n_invwork, st);
-            return;
-        }
         if (P->n_invwork == 0) return;
         dim3 grid(P->n_invwork, (C + InvCfg<T>::CT - 1) / InvCfg<T>::CT);
         k_leg_inv_simt<T><<<grid, 256, P->inv_smem, st>>>(almT, C, spec, P->L, P->M, P->nside, P->d_pairs,
-                                                          P->d_lstart, P->d_pstart, P->d_coef, P->d_invwork);
+                                                          P->d_lstart, P->d_pstart, P->d_coef, P->Lpad,
+                                                          P->d_invwork);
     }
 };
 
@@ -484,6 +594,7 @@ int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void*
                 break;
             }
         }
+        if (pl.rc != HPX_OK) return pl.rc;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return set_err(HPX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     }
@@ -555,7 +666,7 @@ int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
     (void)batch;  // the batch is processed in chunks of batch_chunk maps
     size_t s = ((plan->spec_bytes() + 255) & ~(size_t)255) + ((plan->almT_bytes() + 255) & ~(size_t)255) +
                ((plan->resid_bytes() + 255) & ~(size_t)255);
-    s += tc_workspace_bytes(plan->tc);
+    s += (plan->tcA_bytes() + 255) & ~(size_t)255;
     *bytes = s;
     return HPX_OK;
 }
@@ -582,6 +693,21 @@ int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_gra
 int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, void* ws,
                             size_t ws_bytes, void* stream) {
     return dispatch(plan, kInverseAdjoint, map_grad, alm_grad, batch, ws, ws_bytes, stream);
+}
+
+int hpx_plan_check(hpx_plan_t plan, void* stream) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    if (!plan->tc.d_err) return HPX_OK;
+    DeviceGuard dg(plan->device);
+    int h = 0;
+    HPX_CUDA_TRY(cudaMemcpyAsync(&h, plan->tc.d_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    HPX_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h != 0) {
+        cudaMemsetAsync(plan->tc.d_err, 0, sizeof(int), (cudaStream_t)stream);
+        cudaStreamSynchronize((cudaStream_t)stream);
+        return set_err(HPX_ERR_TIMEOUT, "tensor-core pipeline wait timed out (code " + std::to_string(h) + ")");
+    }
+    return HPX_OK;
 }
 
 int hpx_stats_enable(hpx_plan_t plan, int enable) {

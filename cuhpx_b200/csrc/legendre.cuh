@@ -90,13 +90,16 @@ __device__ __forceinline__ double leg_step(int l, int ls, double2 ps, double a, 
     return v;
 }
 
-// Recurrence coefficients a_lm, b_lm for every (m, l >= m+2), shared by the
-// seed precompute and all contraction kernels: coef[m * L + l] = (a, b).
-__global__ void k_legendre_coef(int M, int L, double2* __restrict__ coef) {
+// Recurrence coefficients a_lm, b_lm for every (m, m+2 <= l < L), shared by the
+// seed precompute and all contraction kernels: coef[m * Lpad + l] = (a, b).
+// Rows are padded to Lpad = L + kCoefPad with zeros, so a recurrence run past
+// l = L-1 yields exact zeros without a branch.
+constexpr int kCoefPad = 256;
+__global__ void k_legendre_coef(int M, int L, int Lpad, double2* __restrict__ coef) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)M * L) return;
-    const int m = (int)(idx / L), l = (int)(idx % L);
-    coef[idx] = l >= m + 2 ? make_double2(rec_a(l, m), rec_b(l, m)) : make_double2(0.0, 0.0);
+    if (idx >= (int64_t)M * Lpad) return;
+    const int m = (int)(idx / Lpad), l = (int)(idx % Lpad);
+    coef[idx] = (l >= m + 2 && l < L) ? make_double2(rec_a(l, m), rec_b(l, m)) : make_double2(0.0, 0.0);
 }
 
 // Degree-block seeds: for every (m, block j, north ring p) the FP64 pair
@@ -106,7 +109,7 @@ constexpr int kSeedBlock = 64;
 
 __host__ __device__ inline int seed_blocks(int L) { return (L + kSeedBlock - 1) / kSeedBlock; }
 
-__global__ void k_legendre_seeds(int M, int L, int nside, const RingPair* __restrict__ pairs,
+__global__ void k_legendre_seeds(int M, int L, int Lpad, int nside, const RingPair* __restrict__ pairs,
                                  const int* __restrict__ lstart, const double2* __restrict__ pstart,
                                  const double2* __restrict__ coef, double2* __restrict__ seeds) {
     const int NP = 2 * nside;
@@ -120,7 +123,7 @@ __global__ void k_legendre_seeds(int M, int L, int nside, const RingPair* __rest
     const double2 ps = pstart[idx];
     const double x = pairs[p].z;
     double p1 = 0.0, p2 = 0.0;
-    const double2* cm = coef + (int64_t)m * L;
+    const double2* cm = coef + (int64_t)m * Lpad;
     for (int l = m; l < L; ++l) {
         double2 ab = l >= m + 2 ? cm[l] : make_double2(0.0, 0.0);
         double v = leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2);
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec
                                                       const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
                                                       const double2* __restrict__ pstart,
-                                                      const double2* __restrict__ coef,
+                                                      const double2* __restrict__ coef, int Lpad,
                                                       const double2* __restrict__ seeds,
                                                       const int2* __restrict__ tiles, int accumulate) {
     using Cfg = FwdCfg<T>;
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec
     if (m >= L) return;
     for (int i = tid; i < LT; i += blockDim.x) {
         const int l = l0 + i;
-        cf[i] = (l < L && l >= m + 2) ? coef[(int64_t)m * L + l] : make_double2(0.0, 0.0);
+        cf[i] = (l < L && l >= m + 2) ? coef[(int64_t)m * Lpad + l] : make_double2(0.0, 0.0);
     }
 
     const int tx = tid & 15, ty = tid >> 4;
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
                                                       int M, int nside, const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
                                                       const double2* __restrict__ pstart,
-                                                      const double2* __restrict__ coef,
+                                                      const double2* __restrict__ coef, int Lpad,
                                                       const int2* __restrict__ work) {
     using Cfg = InvCfg<T>;
     constexpr int RBI = Cfg::RBI, CT = Cfg::CT, LC = Cfg::LC, RBP = Cfg::RBP;
@@ -367,7 +370,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
     const int K = NP - t0;
 
     for (int l = m + 2 + tid; l < L; l += blockDim.x) {
-        const double2 ab = coef[(int64_t)m * L + l];
+        const double2 ab = coef[(int64_t)m * Lpad + l];
         coefA[l] = ab.x;
         coefB[l] = ab.y;
     }

@@ -19,7 +19,8 @@ Differences from the reference, all deliberate:
   pins the stream that was current at construction);
 * gradients are the exact adjoints of the transforms (the reference's
   hand-written backward is approximate, cuhpx/hpx_sht.py:565-583, 614-641);
-* keyword-only extras: ``precision`` ('fp32', 'bf16x3', 'tf32'),
+* keyword-only extras: ``precision`` ('fp32' or 'bf16x3': tcgen05 tensor
+  cores with a three-term bf16 split and FP32 accumulation),
   ``refine_iters`` (Jacobi refinement of the analysis), ``batch_chunk``.
 """
 
@@ -76,6 +77,12 @@ class Plan:
             except Exception:
                 pass
             self._h = None
+
+    def check(self, device=None):
+        """Synchronise and raise if a kernel gave up on a bounded pipeline wait."""
+        dev = torch.device("cuda", self.device) if device is None else device
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(self._lib.hpx_plan_check(self._h, ctypes.c_void_p(stream)), self._h)
 
     # ------------------------------------------------------------------ stats
     def stats_enable(self, on=True):
@@ -223,8 +230,8 @@ class _Base(nn.Module):
         self.quad_weights = quad_weights
         self.lmax = lmax or self.nlat
         self.mmax = mmax or (self.nlon // 2 + 1)
-        if precision not in ("fp32", "bf16x3", "tf32"):
-            raise ValueError("precision must be 'fp32', 'bf16x3' or 'tf32' (float64 data select fp64 automatically)")
+        if precision not in ("fp32", "bf16x3"):
+            raise ValueError("precision must be 'fp32' or 'bf16x3' (float64 data select fp64 automatically)")
         self.precision = precision
         self.refine_iters = int(refine_iters)
         self.batch_chunk = int(batch_chunk)

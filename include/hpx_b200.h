@@ -120,6 +120,10 @@ typedef struct {
 HPX_API int hpx_stats_enable(hpx_plan_t plan, int enable);
 HPX_API int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stages, int* n_stages);
 
+/* Synchronise `stream` and report whether a kernel of this plan gave up on a
+ * bounded pipeline wait since the last check (HPX_ERR_TIMEOUT, flag cleared). */
+HPX_API int hpx_plan_check(hpx_plan_t plan, void* stream);
+
 /* Plan geometry queries. */
 HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);
 
