@@ -6,131 +6,177 @@
 
 namespace hpx {
 
-// Per-m ring-stage scale factors, see the adjoint derivation in hpx_plan.cu.
-enum RingMode : int {
-    kRingPlain = 0,    // forward: S/D weighted by w_t;  inverse: F = E +/- O
-    kRingAdjoint = 1,  // forward-side adjoint of the inverse: weight c_m = 2 (1 at m=0, nphi/2)
-                       // inverse-side adjoint of the forward: scale w_t * c_m/2 (w_t at m=0, nphi/2)
-    kRingResidual = 2  // inverse: write ref - synthesis (Jacobi residual)
-};
-
-template <typename T>
-__host__ __device__ constexpr size_t ring_smem_bytes(int bufP, int mtmax, int nmax) {
-    return ((size_t)bufP + 2 * (size_t)mtmax + 64 + (2 * (size_t)nmax + 63) / 64 + 2) * sizeof(cplx<T>);
+// complex elements of dynamic shared memory the ring kernels need
+__host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
+    return 64 + (2 * (size_t)nmax + 63) / 64 + 2 * (size_t)(pfft_max > 4096 ? pfft_max : 4096);
 }
 
-// map[b][npix] -> spec[m][0|1][p][c]
-// With xh != nullptr (mixed-precision plans) the folded spectra are written as
-// bf16 hi/lo pairs xh/xl[m][par][p][c] instead of T values in spec.
+// One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
 template <typename T>
 __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
-                                                  T* __restrict__ spec, int C, int nside, int mtmax, int bufP,
+                                                  T* __restrict__ F, int64_t Ftot, int nside,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
-                                                  int logPmax, const cplx<T>* __restrict__ gtab, int mode,
-                                                  uint32_t* __restrict__ xh, uint32_t* __restrict__ xl) {
+                                                  int logPmax, const cplx<T>* __restrict__ gtab,
+                                                  const cplx<T>* __restrict__ chirp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NP = 2 * nside;
-    const int p = blockIdx.x;
-    const RingPair rp = pairs[p];
-    cplx<T>* buf = (cplx<T>*)smem_raw;
-    cplx<T>* Fn = buf + bufP;
-    cplx<T>* Fs = Fn + mtmax;
-    cplx<T>* elo = Fs + mtmax;
+    const int NP = 2 * nside, R = 4 * nside - 1;
+    const int t = blockIdx.x;
+    const bool south = t >= NP;
+    const RingPair rp = pairs[south ? R - 1 - t : t];
+    cplx<T>* elo = (cplx<T>*)smem_raw;
     cplx<T>* ehi = elo + 64;
+    cplx<T>* bufs = ehi + (2 * rp.nphi + 63) / 64;
     build_phase_tab(elo, ehi, rp.nphi);
     __syncthreads();
-    const PhaseTab<T> E{elo, ehi, 2 * rp.nphi};
+    const PhaseTab<T> E{elo, ehi};
+    const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
+    const int P = 1 << rp.logP;
+    cplx<T>* buf = bufs + (size_t)g * 2 * P;
+    cplx<T>* buf2 = buf + P;
+    const int64_t start = south ? rp.start_s : rp.start_n;
+    const int64_t foff = south ? rp.foff_s : rp.foff_n;
+    const int shift = south ? rp.shift_s : rp.shift_n;
     const int64_t np = npix(nside);
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
-    for (int b = b0; b < b1; ++b) {
-        const T* mp = map + (int64_t)b * np;
-        ring_forward(mp + rp.start_n, rp.shift_n, buf, Fn, rp, tw, logPmax, gtab, E);
-        __syncthreads();
+    for (int b = b0 + g; b < b1; b += S)
+        ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff), rp, tw,
+                     logPmax, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+}
+
+// One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
+// (ref != nullptr: write ref - synthesis)
+template <typename T>
+__global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map,
+                                                  int nmaps, int maps_per_cta, int nside,
+                                                  const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
+                                                  int logPmax, const cplx<T>* __restrict__ gtab,
+                                                  const cplx<T>* __restrict__ chirp, const T* __restrict__ ref) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int NP = 2 * nside, R = 4 * nside - 1;
+    const int t = blockIdx.x;
+    const bool south = t >= NP;
+    const RingPair rp = pairs[south ? R - 1 - t : t];
+    cplx<T>* elo = (cplx<T>*)smem_raw;
+    cplx<T>* ehi = elo + 64;
+    cplx<T>* bufs = ehi + (2 * rp.nphi + 63) / 64;
+    build_phase_tab(elo, ehi, rp.nphi);
+    __syncthreads();
+    const PhaseTab<T> E{elo, ehi};
+    const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
+    const int P = 1 << rp.logP;
+    cplx<T>* buf = bufs + (size_t)g * 2 * P;
+    cplx<T>* buf2 = buf + P;
+    const int64_t start = south ? rp.start_s : rp.start_n;
+    const int64_t foff = south ? rp.foff_s : rp.foff_n;
+    const int shift = south ? rp.shift_s : rp.shift_n;
+    const int64_t np = npix(nside);
+    const int b0 = blockIdx.y * maps_per_cta;
+    const int b1 = min(b0 + maps_per_cta, nmaps);
+    for (int b = b0 + g; b < b1; b += S)
+        ring_inverse((const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + foff)), shift, buf, buf2,
+                     map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr, rp, tw, logPmax,
+                     gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+}
+
+// Fold ring spectra into the m-major Legendre operand:
+//   S = c (F_t + F_t'),  D = c (F_t - F_t')   (equator: S = c F_t, D = 0)
+// with c = w_t (analysis) or c_m = 2, 1 at m = 0 and m = nphi/2 (adjoint of synthesis).
+// Output spec[m][par][p][col] in T, or bf16 hi/lo pairs xh/xl (mixed plans).
+// CTA per (block of 32 orders, ring pair); the transpose goes through shared memory.
+template <typename T>
+constexpr int fold_mb() { return sizeof(T) == 4 ? 32 : 16; }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t Ftot, int nmaps, int nside,
+                                              const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ spec,
+                                              int C, uint32_t* __restrict__ xh, uint32_t* __restrict__ xl) {
+    constexpr int MB = fold_mb<T>();
+    __shared__ cplx<T> tn[64][MB + 1];
+    __shared__ cplx<T> ts[64][MB + 1];
+    const int NP = 2 * nside;
+    const int m0 = blockIdx.x * MB, p = blockIdx.y, bz = blockIdx.z * 64;
+    const RingPair rp = pairs[p];
+    if (m0 >= rp.mt) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 64 * MB; i += blockDim.x) {
+        const int b = bz + i / MB, mm = i % MB, m = m0 + mm;
+        cplx<T> vn = {(T)0, (T)0}, vs = {(T)0, (T)0};
+        if (b < nmaps && m < rp.mt) {
+            vn = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m));
+            if (rp.has_south) vs = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m));
+        }
+        tn[b - bz][mm] = vn;
+        ts[b - bz][mm] = vs;
+    }
+    __syncthreads();
+    // each thread: one (m, map) pair -> S and D
+    for (int i = tid; i < MB * 64; i += blockDim.x) {
+        const int mm = i >> 6, bl = i & 63, b = bz + bl, m = m0 + mm;
+        if (m >= rp.mt || 2 * b >= C) continue;
+        const T wk = adjoint ? ((m == 0 || m == rp.h) ? (T)1 : (T)2) : (T)rp.w;
+        const cplx<T> a = tn[bl][mm], c = ts[bl][mm];
+        cplx<T> S, D;
         if (rp.has_south) {
-            ring_forward(mp + rp.start_s, rp.shift_s, buf, Fs, rp, tw, logPmax, gtab, E);
-            __syncthreads();
+            S = cscale(cadd(a, c), wk);
+            D = cscale(csub(a, c), wk);
+        } else {
+            S = cscale(a, wk);
+            D = {(T)0, (T)0};
         }
-        for (int k = threadIdx.x; k < rp.mt; k += blockDim.x) {
-            T wk;
-            if (mode == kRingAdjoint) wk = (k == 0 || k == rp.h) ? (T)1 : (T)2;
-            else wk = (T)rp.w;
-            cplx<T> S, D;
-            if (rp.has_south) {
-                S = cscale(cadd(Fn[k], Fs[k]), wk);
-                D = cscale(csub(Fn[k], Fs[k]), wk);
-            } else {
-                S = cscale(Fn[k], wk);
-                D = {(T)0, (T)0};
-            }
-            const int64_t i0 = (((int64_t)k * 2 + 0) * NP + p) * C + 2 * b;
-            const int64_t i1 = (((int64_t)k * 2 + 1) * NP + p) * C + 2 * b;
-            if (xh) {
-                uint16_t h0, l0, h1, l1;
-                tc::split_bf16((float)S.re, h0, l0);
-                tc::split_bf16((float)S.im, h1, l1);
-                xh[i0 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-                xl[i0 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
-                tc::split_bf16((float)D.re, h0, l0);
-                tc::split_bf16((float)D.im, h1, l1);
-                xh[i1 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-                xl[i1 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
-            } else {
-                *(cplx<T>*)(spec + i0) = S;
-                *(cplx<T>*)(spec + i1) = D;
-            }
+        const int64_t i0 = (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b;
+        const int64_t i1 = (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b;
+        if (xh) {
+            uint16_t h0, l0, h1, l1;
+            tc::split_bf16((float)S.re, h0, l0);
+            tc::split_bf16((float)S.im, h1, l1);
+            xh[i0 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+            xl[i0 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+            tc::split_bf16((float)D.re, h0, l0);
+            tc::split_bf16((float)D.im, h1, l1);
+            xh[i1 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+            xl[i1 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+        } else {
+            *(cplx<T>*)(spec + i0) = S;
+            *(cplx<T>*)(spec + i1) = D;
         }
-        __syncthreads();
     }
 }
 
-// spec[m][0|1][p][c] -> map[b][npix]
+// Unfold the synthesis output spec[m][par][p][col] (E = even, O = odd degrees)
+// into ring spectra F_t = sc (E + O), F_t' = sc (E - O), with sc = 1, or for
+// the adjoint of analysis sc = w_t (m = 0, nphi/2) and w_t/2 otherwise.
 template <typename T>
-__global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ spec, int C, T* __restrict__ map, int nmaps,
-                                                  int maps_per_cta, int nside, int mtmax, int bufP,
-                                                  const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
-                                                  int logPmax, const cplx<T>* __restrict__ gtab, int mode,
-                                                  const T* __restrict__ ref) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int C, int nmaps, int nside,
+                                                const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ F,
+                                                int64_t Ftot) {
+    constexpr int MB = fold_mb<T>();
+    __shared__ cplx<T> te[MB][65];
+    __shared__ cplx<T> to[MB][65];
     const int NP = 2 * nside;
-    const int p = blockIdx.x;
+    const int m0 = blockIdx.x * MB, p = blockIdx.y, bz = blockIdx.z * 64;
     const RingPair rp = pairs[p];
-    cplx<T>* buf = (cplx<T>*)smem_raw;
-    cplx<T>* Fn = buf + bufP;
-    cplx<T>* Fs = Fn + mtmax;
-    cplx<T>* elo = Fs + mtmax;
-    cplx<T>* ehi = elo + 64;
-    build_phase_tab(elo, ehi, rp.nphi);
+    if (m0 >= rp.mt) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < MB * 64; i += blockDim.x) {
+        const int mm = i >> 6, bl = i & 63, b = bz + bl, m = m0 + mm;
+        cplx<T> e = {(T)0, (T)0}, o = {(T)0, (T)0};
+        if (m < rp.mt && 2 * b < C) {
+            e = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b);
+            o = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b);
+        }
+        te[mm][bl] = e;
+        to[mm][bl] = o;
+    }
     __syncthreads();
-    const PhaseTab<T> E{elo, ehi, 2 * rp.nphi};
-    const int64_t np = npix(nside);
-    const int b0 = blockIdx.y * maps_per_cta;
-    const int b1 = min(b0 + maps_per_cta, nmaps);
-    for (int b = b0; b < b1; ++b) {
-        for (int k = threadIdx.x; k < rp.mt; k += blockDim.x) {
-            cplx<T> e = *(const cplx<T>*)(spec + (((int64_t)k * 2 + 0) * NP + p) * C + 2 * b);
-            cplx<T> o = *(const cplx<T>*)(spec + (((int64_t)k * 2 + 1) * NP + p) * C + 2 * b);
-            T sc = (T)1;
-            if (mode == kRingAdjoint) sc = (k == 0 || k == rp.h) ? (T)rp.w : (T)(0.5 * rp.w);
-            Fn[k] = cscale(cadd(e, o), sc);
-            Fs[k] = cscale(csub(e, o), sc);
-        }
-        __syncthreads();
-        T* mp = map + (int64_t)b * np;
-        ring_inverse(Fn, rp.shift_n, buf, mp + rp.start_n, rp, tw, logPmax, gtab, E);
-        __syncthreads();
-        if (rp.has_south) {
-            ring_inverse(Fs, rp.shift_s, buf, mp + rp.start_s, rp, tw, logPmax, gtab, E);
-            __syncthreads();
-        }
-        if (mode == kRingResidual) {
-            const T* rf = ref + (int64_t)b * np;
-            for (int j = threadIdx.x; j < rp.nphi; j += blockDim.x) {
-                mp[rp.start_n + j] = rf[rp.start_n + j] - mp[rp.start_n + j];
-                if (rp.has_south) mp[rp.start_s + j] = rf[rp.start_s + j] - mp[rp.start_s + j];
-            }
-            __syncthreads();
-        }
+    for (int i = tid; i < 64 * MB; i += blockDim.x) {
+        const int bl = i / MB, mm = i % MB, b = bz + bl, m = m0 + mm;
+        if (b >= nmaps || m >= rp.mt) continue;
+        T sc = (T)1;
+        if (adjoint) sc = (m == 0 || m == rp.h) ? (T)rp.w : (T)(0.5 * rp.w);
+        const cplx<T> e = te[mm][bl], o = to[mm][bl];
+        *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m)) = cscale(cadd(e, o), sc);
+        if (rp.has_south) *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m)) = cscale(csub(e, o), sc);
     }
 }
 
@@ -158,33 +204,36 @@ __global__ void k_alm_to_cols(const T* __restrict__ alm, int nmaps, int L, int M
     }
 }
 
-// Bluestein chirp spectra: G_p = FFT_P(g) / P stored bit-reversed, g_j = e^{+i pi j^2/h}
-// for |j| < h (circularly wrapped), computed in FP64 and rounded to T.
+// Bluestein tables per ring pair (FP64, rounded to T):
+//   chirp[j] = e^{-i pi j^2/h}, j < h  (phase from the integer j^2 mod 2h)
+//   G = FFT_P(g) / P in natural order, g_j = e^{+i pi j^2/h} for |j| < h (wrapped)
 template <typename T>
 __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restrict__ pairs,
                                                        const cplx<double>* __restrict__ tw64, int logPmax,
-                                                       cplx<T>* __restrict__ gtab) {
+                                                       cplx<T>* __restrict__ gtab, cplx<T>* __restrict__ chirp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const RingPair rp = pairs[blockIdx.x];
     if (rp.logh >= 0) return;
     cplx<double>* buf = (cplx<double>*)smem_raw;
+    cplx<double>* buf2 = buf + (1 << rp.logP);
     const int P = 1 << rp.logP, h = rp.h;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
-        int d = j < h ? j : (j > P - h ? P - j : -1);
+        const int d = j < h ? j : (j > P - h ? P - j : -1);
         cplx<double> v = {0.0, 0.0};
         if (d >= 0) {
-            long long q = ((long long)d * d) % (2 * h);
+            const long long q = ((long long)d * d) % (2 * h);
             double s, c;
             sincospi((double)q / (double)h, &s, &c);
             v = {c, s};
         }
         buf[j] = v;
+        if (j < h) chirp[rp.gtab_off + j] = {(T)v.re, (T)(-v.im)};
     }
     __syncthreads();
-    fft_dif(buf, rp.logP, tw64, logPmax, false);
+    cplx<double>* r = stockham<double, false>(buf, buf2, rp.logP, tw64, logPmax, threadIdx.x, blockDim.x, 0);
     const double inv = 1.0 / (double)P;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
-        gtab[rp.gtab_off + j] = {(T)(buf[j].re * inv), (T)(buf[j].im * inv)};
+        gtab[rp.gtab_off + j] = {(T)(r[j].re * inv), (T)(r[j].im * inv)};
     }
 }
 

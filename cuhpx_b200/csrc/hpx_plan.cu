@@ -67,9 +67,9 @@ int ceil_log2(int v) {
     return r;
 }
 
-enum Stage { kStRingFwd = 0, kStRingInv, kStLegFwd, kStLegInv, kStAlmCols, kNumStages };
-const char* kStageNames[kNumStages] = {"ring_fft_forward", "ring_fft_inverse", "legendre_forward",
-                                       "legendre_inverse", "alm_to_columns"};
+enum Stage { kStRingFwd = 0, kStRingInv, kStLegFwd, kStLegInv, kStAlmCols, kStFold, kStUnfold, kNumStages };
+const char* kStageNames[kNumStages] = {"ring_fft_forward", "ring_fft_inverse", "legendre_forward", "legendre_inverse",
+                                       "alm_to_columns",   "fold",             "unfold"};
 
 }  // namespace
 
@@ -88,7 +88,9 @@ struct hpx_plan_s {
     std::vector<RingPair> h_pairs;
     RingPair* d_pairs = nullptr;
     void* d_tw = nullptr;   // cplx<T> twiddles for the plan's FFT type
-    void* d_gtab = nullptr; // cplx<T> chirp spectra
+    void* d_gtab = nullptr; // cplx<T> Bluestein chirp spectra (natural order)
+    void* d_chirp = nullptr; // cplx<T> Bluestein chirps
+    int64_t Ftot = 0;        // complex spectrum entries per map over all rings
     int* d_lstart = nullptr;
     double2* d_pstart = nullptr;
     int2* d_invwork = nullptr;
@@ -131,6 +133,7 @@ struct hpx_plan_s {
         cudaFree(d_pairs);
         cudaFree(d_tw);
         cudaFree(d_gtab);
+        cudaFree(d_chirp);
         cudaFree(d_lstart);
         cudaFree(d_pstart);
         cudaFree(d_invwork);
@@ -153,6 +156,7 @@ struct hpx_plan_s {
     size_t spec_bytes() const { return (size_t)M * 2 * NP * cols() * real_size(); }
     size_t almT_bytes() const { return (size_t)M * L * cols() * real_size(); }
     size_t resid_bytes() const { return (size_t)batch_chunk * npix * real_size(); }
+    size_t F_bytes() const { return (size_t)batch_chunk * Ftot * 2 * real_size(); }
     bool mixed() const { return prec == HPX_PREC_BF16X3; }
     // bf16 hi/lo synthesis operand [2M][Lh][128] x 2
     size_t tcA_bytes() const { return mixed() ? (size_t)2 * 2 * M * tc.Lh * kTcCols * sizeof(uint16_t) : 0; }
@@ -189,12 +193,13 @@ int create_typed(hpx_plan_s* P) {
         HPX_CUDA_TRY(cudaMalloc(&tw64, (size_t)(Pmax / 2) * sizeof(cplx<double>)));
         k_twiddles<double><<<(Pmax / 2 + 255) / 256, 256>>>(tw64, Pmax);
         HPX_CUDA_TRY(cudaMalloc(&P->d_gtab, (size_t)gsize * sizeof(C)));
-        size_t sm = (size_t)Pmax * sizeof(cplx<double>);
+        HPX_CUDA_TRY(cudaMalloc(&P->d_chirp, (size_t)gsize * sizeof(C)));
+        size_t sm = (size_t)2 * Pmax * sizeof(cplx<double>);
         int dmax = 0;
         HPX_CUDA_TRY(cudaDeviceGetAttribute(&dmax, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
         if ((int)sm > dmax) return set_err(HPX_ERR_UNSUPPORTED, "nside too large for the chirp precompute");
         HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmax));
-        k_chirp_spectra<T><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab);
+        k_chirp_spectra<T><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab, (C*)P->d_chirp);
         cudaError_t e = cudaGetLastError();
         cudaError_t e2 = cudaDeviceSynchronize();
         cudaFree(tw64);
@@ -202,7 +207,7 @@ int create_typed(hpx_plan_s* P) {
             return set_err(HPX_ERR_CUDA, std::string("chirp spectra: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
     // shared memory budgets
-    P->ring_smem = ring_smem_bytes<T>(P->bufP, P->mtmax, P->nmax);
+    P->ring_smem = ring_smem_elems(P->bufP, P->nmax) * sizeof(C);
     P->fwd_smem = fwd_smem_bytes<T>();
     P->inv_smem = inv_smem_bytes<T>(P->L);
     int dev_max = 0;
@@ -305,6 +310,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     const double four_pi_over_npix = 4.0 * M_PI / (double)P->npix;
     for (int p = 0; p < P->NP; ++p) {
         RingPair& rp = P->h_pairs[p];
+        std::memset(&rp, 0, sizeof(rp));
         const int ts = 4 * N - 2 - p;
         rp.nphi = ring_nphi(p, N);
         rp.h = rp.nphi / 2;
@@ -320,19 +326,29 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
         else rp.w = four_pi_over_npix;
         rp.logh = ilog2_exact(rp.h);
         if (rp.logh >= 0) {
-            rp.logP = 0;
+            rp.logP = rp.logh;
             rp.gtab_off = -1;
-            logPmax = std::max(logPmax, std::max(rp.logh, 1));
-            bufP = std::max(bufP, rp.h);
         } else {
             rp.logP = ceil_log2(2 * rp.h - 1);
             rp.gtab_off = goff;
             goff += 1ll << rp.logP;
-            logPmax = std::max(logPmax, rp.logP);
-            bufP = std::max(bufP, 1 << rp.logP);
         }
+        const int Pf = 1 << rp.logP;
+        logPmax = std::max(logPmax, std::max(rp.logP, 1));
+        bufP = std::max(bufP, Pf);
+        // threads per FFT: ~16 points per thread, between one warp and the CTA
+        rp.tpf = std::min(256, std::max(32, Pf / 16));
         mtmax = std::max(mtmax, rp.mt);
     }
+    // ring-major spectrum offsets: north rings 0..NP-1, then south rings
+    int64_t foff = 0;
+    for (int t = 0; t < P->R; ++t) {
+        const bool south = t >= P->NP;
+        RingPair& rp = P->h_pairs[south ? P->R - 1 - t : t];
+        if (south) rp.foff_s = foff; else rp.foff_n = foff;
+        foff += rp.mt;
+    }
+    P->Ftot = foff;
     P->logPmax = logPmax;
     P->bufP = bufP;
     P->mtmax = mtmax;
@@ -447,14 +463,16 @@ struct Pipeline {
         resid = (T*)c;
         c += (P->resid_bytes() + 255) & ~(size_t)255;
         tcA = (uint16_t*)c;
+        c += (P->tcA_bytes() + 255) & ~(size_t)255;
+        F = (T*)c;
     }
+    T* F;  // ring-major spectra [map][Ftot] complex
     // folded spectra as bf16 hi/lo (mixed plans), aliasing the spec region
     uint32_t* xh() const { return P->mixed() ? (uint32_t*)spec : nullptr; }
     uint32_t* xl() const {
         return P->mixed() ? (uint32_t*)((uint16_t*)spec + (size_t)2 * P->M * P->NP * kTcCols) : nullptr;
     }
 
-    int maps_per_cta(int nb) const { return std::min(nb, 4); }
 
     // brackets one launch with events when the plan's stats are enabled
     struct Timer {
@@ -477,21 +495,35 @@ struct Pipeline {
         }
     };
 
-    void ring_fwd(const T* map, int nb, int mode) {
-        const int g = maps_per_cta(nb);
-        dim3 grid(P->NP, (nb + g - 1) / g);
-        Timer tm(P, st, kStRingFwd);
-        k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, spec, P->cols(), P->nside, P->mtmax, P->bufP,
-                                                      P->d_pairs, (const cplx<T>*)P->d_tw, P->logPmax,
-                                                      (const cplx<T>*)P->d_gtab, mode, xh(), xl());
+    int maps_per_cta_ring() const { return 8; }
+
+    // map -> ring spectra F -> folded Legendre operand (spec, or bf16 hi/lo)
+    void ring_fwd(const T* map, int nb, int adjoint) {
+        const int g = maps_per_cta_ring();
+        {
+            Timer tm(P, st, kStRingFwd);
+            dim3 grid(P->R, (nb + g - 1) / g);
+            k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->nside, P->d_pairs,
+                                                          (const cplx<T>*)P->d_tw, P->logPmax,
+                                                          (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp);
+        }
+        Timer tm(P, st, kStFold);
+        dim3 fg((P->mtmax + fold_mb<T>() - 1) / fold_mb<T>(), P->NP, (nb + 63) / 64);
+        k_fold<T><<<fg, 256, 0, st>>>(F, P->Ftot, nb, P->nside, P->d_pairs, adjoint, spec, P->cols(), xh(), xl());
     }
-    void ring_inv(T* map, int nb, int mode, const T* ref) {
-        const int g = maps_per_cta(nb);
-        dim3 grid(P->NP, (nb + g - 1) / g);
+    // synthesis output spec (E/O) -> ring spectra F -> map (ref: residual ref - map)
+    void ring_inv(T* map, int nb, int adjoint, const T* ref) {
+        {
+            Timer tm(P, st, kStUnfold);
+            dim3 fg((P->mtmax + fold_mb<T>() - 1) / fold_mb<T>(), P->NP, (nb + 63) / 64);
+            k_unfold<T><<<fg, 256, 0, st>>>(spec, P->cols(), nb, P->nside, P->d_pairs, adjoint, F, P->Ftot);
+        }
+        const int g = maps_per_cta_ring();
         Timer tm(P, st, kStRingInv);
-        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(spec, P->cols(), map, nb, g, P->nside, P->mtmax, P->bufP,
-                                                      P->d_pairs, (const cplx<T>*)P->d_tw, P->logPmax,
-                                                      (const cplx<T>*)P->d_gtab, mode, ref);
+        dim3 grid(P->R, (nb + g - 1) / g);
+        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(F, P->Ftot, map, nb, g, P->nside, P->d_pairs,
+                                                      (const cplx<T>*)P->d_tw, P->logPmax, (const cplx<T>*)P->d_gtab,
+                                                      (const cplx<T>*)P->d_chirp, ref);
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();
@@ -567,7 +599,7 @@ int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void*
             case kInverseAdjoint: {
                 const T* map = (const T*)in + b0 * P->npix;
                 T* alm = (T*)out + b0 * alm_stride;
-                pl.ring_fwd(map, nb, op == kForward ? kRingPlain : kRingAdjoint);
+                pl.ring_fwd(map, nb, op == kForward ? 0 : 1);
                 pl.leg_fwd(alm, nb, 0);
                 break;
             }
@@ -575,12 +607,12 @@ int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void*
                 // a = S f;  repeat: r = f - I a;  a += S r
                 const T* map = (const T*)in + b0 * P->npix;
                 T* alm = (T*)out + b0 * alm_stride;
-                pl.ring_fwd(map, nb, kRingPlain);
+                pl.ring_fwd(map, nb, 0);
                 pl.leg_fwd(alm, nb, 0);
                 for (int it = 0; it < iters; ++it) {
                     pl.leg_inv(alm, nb);
-                    pl.ring_inv(pl.resid, nb, kRingResidual, map);
-                    pl.ring_fwd(pl.resid, nb, kRingPlain);
+                    pl.ring_inv(pl.resid, nb, 0, map);
+                    pl.ring_fwd(pl.resid, nb, 0);
                     pl.leg_fwd(alm, nb, 1);
                 }
                 break;
@@ -590,7 +622,7 @@ int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void*
                 const T* alm = (const T*)in + b0 * alm_stride;
                 T* map = (T*)out + b0 * P->npix;
                 pl.leg_inv(alm, nb);
-                pl.ring_inv(map, nb, op == kInverse ? kRingPlain : kRingAdjoint, nullptr);
+                pl.ring_inv(map, nb, op == kInverse ? 0 : 1, nullptr);
                 break;
             }
         }
@@ -667,6 +699,7 @@ int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
     size_t s = ((plan->spec_bytes() + 255) & ~(size_t)255) + ((plan->almT_bytes() + 255) & ~(size_t)255) +
                ((plan->resid_bytes() + 255) & ~(size_t)255);
     s += (plan->tcA_bytes() + 255) & ~(size_t)255;
+    s += (plan->F_bytes() + 255) & ~(size_t)255;
     *bytes = s;
     return HPX_OK;
 }

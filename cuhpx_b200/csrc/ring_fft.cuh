@@ -8,22 +8,23 @@
 //   f_p = Re X_0 + 2 sum_{0<m<nphi/2} Re(X_m e^{2 pi i m p/nphi}) + Re X_{nphi/2} (-1)^p,
 //   X_m = e^{+i m phi0_t} F_t[m] for m < min(M, nphi/2+1), 0 above.
 //
-// Design (not the reference's): one CTA owns a ring pair (north ring t and its
-// mirror) for a group of maps.  A real ring of length n = nphi is packed into
-// a complex sequence of length h = n/2; if h is a power of two it goes through
-// a radix-2 FFT in shared memory, otherwise through Bluestein's chirp-z
-// convolution with a per-ring power-of-two size P >= 2h-1 (the reference pads
-// every ring to 8*nside).  Every rotation factor is e^{-i pi q / n} for an
-// integer q reduced mod 2n -- the phase shift (q = s*m), the real-FFT split
-// (q = 2m) and the Bluestein chirp (q = 2 j^2 mod 2n) -- so phases are exact
-// integer reductions evaluated from a per-CTA FP64-built table, never a float
-// "pi*j*j/n" as in hpx_fft_cuda.cu:1090.
+// Design (not the reference's): a real ring of length n = nphi is packed into
+// a complex sequence of length h = n/2.  If h is a power of two it goes
+// through a Stockham radix-4/2 FFT in shared memory, otherwise through
+// Bluestein's chirp-z convolution with a per-ring power-of-two size
+// P >= 2h-1 (the reference pads every ring to 8*nside).  Small rings are
+// transformed by sub-groups of a CTA (one warp, two, four or all eight) so
+// that every thread handles ~16 points whatever the ring length.
 //
-// The forward stage writes the north/south folded, quadrature-weighted spectra
-//   S_t[m] = w_t (F_t[m] + F_t'[m]),  D_t[m] = w_t (F_t[m] - F_t'[m])
-// (equator: S = w F, D = 0) into spec[m][0|1][p][c] with c = 2*map + {re,im};
-// the inverse stage reads E/O = spec[m][0|1][p][c] and unfolds
-// F_t = E + O, F_t' = E - O.
+// Phases are exact: the chirp e^{-i pi j^2/h} is tabulated per ring in the plan
+// from the integer j^2 mod 2h in FP64, and the real-FFT split and phase-shift
+// factors e^{-i pi q/n} (q <= 2n) come from a per-CTA FP64-built table --
+// never from a float "pi*j*j/n" as in hpx_fft_cuda.cu:1090.
+//
+// Spectra are stored ring-major, F[map][foff_t + m] (m < mt_t), so every ring
+// reads and writes contiguous memory; separate fold/unfold kernels (in
+// hpx_kernels.cuh) transpose to and from the m-major layout of the Legendre
+// stage.
 #pragma once
 
 #include "hpx_common.cuh"
@@ -37,74 +38,112 @@ struct RingPair {
     int shift_n;    // phi0 = shift * pi / nphi for the north ring
     int shift_s;    // ... and for the south ring
     int logh;       // log2(h) when h is a power of two, else -1
-    int logP;       // Bluestein FFT size (log2), 0 when direct
+    int logP;       // log2 of the FFT length actually run (h or the Bluestein size)
+    int tpf;        // threads per FFT (32 .. 256)
     int has_south;  // 0 for the equator
-    int64_t start_n;
-    int64_t start_s;
-    int64_t gtab_off;  // offset (complex elements) of the chirp spectrum, -1 if direct
+    int pad_;
+    int64_t start_n;   // first pixel of the north ring
+    int64_t start_s;   // first pixel of the south ring
+    int64_t foff_n;    // spectrum offset of the north ring in F[map][.]
+    int64_t foff_s;    // ... of the south ring
+    int64_t gtab_off;  // offset of the chirp spectrum / chirp (complex elements), -1 if direct
     double z;          // cos(theta) of the north ring
     double w;          // quadrature weight of the ring
 };
 
-// ----------------------------------------------------------------- smem FFTs
-// tw[q] = e^{-2 pi i q / Pmax}, q < Pmax/2
-template <typename T>
-__device__ __forceinline__ cplx<T> twiddle(const cplx<T>* __restrict__ tw, int q, bool inv) {
-    cplx<T> w = tw[q];
-    if (inv) w.im = -w.im;
-    return w;
-}
-
-// natural order in, bit-reversed order out; sum_j a_j e^{-/+ 2 pi i j k / P}
-template <typename T>
-__device__ void fft_dif(cplx<T>* a, int logP, const cplx<T>* __restrict__ tw, int logPmax, bool inv) {
-    const int P2 = 1 << (logP - 1);
-    for (int s = logP; s >= 1; --s) {
-        const int half = 1 << (s - 1);
-        for (int b = threadIdx.x; b < P2; b += blockDim.x) {
-            int j = b & (half - 1);
-            int i0 = ((b >> (s - 1)) << s) + j;
-            int i1 = i0 + half;
-            cplx<T> u = a[i0], v = a[i1];
-            a[i0] = cadd(u, v);
-            a[i1] = cmul(csub(u, v), twiddle(tw, j << (logPmax - s), inv));
-        }
+// ----------------------------------------------------------------- sync helpers
+// Threads [g*tpf, (g+1)*tpf) of the CTA form FFT group g.
+__device__ __forceinline__ void group_sync(int tpf, int g) {
+    if (tpf >= (int)blockDim.x) {
         __syncthreads();
+    } else if (tpf == 32) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(1 + g), "r"(tpf) : "memory");
     }
 }
 
-// bit-reversed order in, natural order out
+// tw[q] = e^{-2 pi i q / Pmax} for q < Pmax/2; the other half by symmetry
 template <typename T>
-__device__ void fft_dit(cplx<T>* a, int logP, const cplx<T>* __restrict__ tw, int logPmax, bool inv) {
-    const int P2 = 1 << (logP - 1);
-    for (int s = 1; s <= logP; ++s) {
-        const int half = 1 << (s - 1);
-        for (int b = threadIdx.x; b < P2; b += blockDim.x) {
-            int j = b & (half - 1);
-            int i0 = ((b >> (s - 1)) << s) + j;
-            int i1 = i0 + half;
-            cplx<T> u = a[i0];
-            cplx<T> v = cmul(a[i1], twiddle(tw, j << (logPmax - s), inv));
-            a[i0] = cadd(u, v);
-            a[i1] = csub(u, v);
-        }
-        __syncthreads();
-    }
+__device__ __forceinline__ cplx<T> twid(const cplx<T>* __restrict__ tw, int q, int half) {
+    if (q < half) return tw[q];
+    cplx<T> v = tw[q - half];
+    return {-v.re, -v.im};
 }
 
-__device__ __forceinline__ int bitrev(int x, int bits) { return bits == 0 ? 0 : (int)(__brev((unsigned)x) >> (32 - bits)); }
+// Stockham autosort radix-4/2 FFT of length P = 2^logP on src (natural order);
+// returns the buffer (src or dst) that holds the natural-order result.
+// INV: e^{+2 pi i jk/P} (unnormalised).  Threads: lt in [0, tpf) of group g.
+template <typename T, bool INV>
+__device__ cplx<T>* stockham(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ tw, int logPmax,
+                             int lt, int tpf, int g) {
+    const int P = 1 << logP;
+    const int half = 1 << (logPmax - 1);
+    int Ns = 1;
+    int rem = logP;
+    while (rem > 0) {
+        if (rem >= 2) {
+            const int Q = P >> 2;
+            const int step = (1 << logPmax) / (Ns * 4);  // twiddle index stride
+            for (int j = lt; j < Q; j += tpf) {
+                const int k = j & (Ns - 1);
+                cplx<T> v0 = src[j], v1 = src[j + Q], v2 = src[j + 2 * Q], v3 = src[j + 3 * Q];
+                if (Ns > 1) {
+                    cplx<T> w1 = twid(tw, k * step, half), w2 = twid(tw, 2 * k * step, half),
+                            w3 = twid(tw, 3 * k * step, half);
+                    if (INV) {
+                        w1.im = -w1.im;
+                        w2.im = -w2.im;
+                        w3.im = -w3.im;
+                    }
+                    v1 = cmul(v1, w1);
+                    v2 = cmul(v2, w2);
+                    v3 = cmul(v3, w3);
+                }
+                const cplx<T> t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
+                const cplx<T> d = csub(v1, v3);
+                // forward: -i*d ; inverse: +i*d
+                const cplx<T> t3 = INV ? cplx<T>{-d.im, d.re} : cplx<T>{d.im, -d.re};
+                const int o = ((j - k) << 2) + k;
+                dst[o] = cadd(t0, t2);
+                dst[o + Ns] = cadd(t1, t3);
+                dst[o + 2 * Ns] = csub(t0, t2);
+                dst[o + 3 * Ns] = csub(t1, t3);
+            }
+            Ns <<= 2;
+            rem -= 2;
+        } else {
+            const int Q = P >> 1;
+            const int step = (1 << logPmax) / (Ns * 2);
+            for (int j = lt; j < Q; j += tpf) {
+                const int k = j & (Ns - 1);
+                cplx<T> v0 = src[j], v1 = src[j + Q];
+                if (Ns > 1) {
+                    cplx<T> w = twid(tw, k * step, half);
+                    if (INV) w.im = -w.im;
+                    v1 = cmul(v1, w);
+                }
+                const int o = ((j - k) << 1) + k;
+                dst[o] = cadd(v0, v1);
+                dst[o + Ns] = csub(v0, v1);
+            }
+            Ns <<= 1;
+            rem -= 1;
+        }
+        group_sync(tpf, g);
+        cplx<T>* t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
 
-// e^{-i pi q / n} from two small tables: q = 64*hi + lo
+// e^{-i pi q / n} for 0 <= q < 2n from two small tables: q = 64*hi + lo
 template <typename T>
 struct PhaseTab {
     const cplx<T>* lo;  // 64 entries
     const cplx<T>* hi;  // ceil(2n/64) entries
-    int two_n;
-    __device__ __forceinline__ cplx<T> operator()(int q) const {
-        q %= two_n;
-        if (q < 0) q += two_n;
-        return cmul(hi[q >> 6], lo[q & 63]);
-    }
+    __device__ __forceinline__ cplx<T> operator()(int q) const { return cmul(hi[q >> 6], lo[q & 63]); }
 };
 
 template <typename T>
@@ -119,103 +158,104 @@ __device__ void build_phase_tab(cplx<T>* lo, cplx<T>* hi, int n) {
     }
 }
 
-// Complex DFT of length h held in buf: fwd computes sum_j z_j e^{-2 pi i jk/h}.
-// Input z must already be in buf (natural order, h entries).  Result is
-// returned through get(k) semantics: after the call, zget(buf, k) gives Z_k.
-//   direct (logh >= 0): result in bit-reversed order
-//   Bluestein: result in natural order, multiplied by chirp on read
+// Complex DFT of length h of buf (natural order, h entries written by this
+// group), forward (e^-) or inverse (e^+); returns the buffer with Z in natural order.
 template <typename T>
-__device__ void ring_dft(cplx<T>* buf, const RingPair& rp, const cplx<T>* __restrict__ tw, int logPmax,
-                         const cplx<T>* __restrict__ gtab, const PhaseTab<T>& E, bool inv) {
+__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const cplx<T>* __restrict__ tw,
+                             int logPmax, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+                             bool inv, int lt, int tpf, int g) {
+    group_sync(tpf, g);
     if (rp.logh >= 0) {
-        __syncthreads();
-        if (rp.logh > 0) fft_dif(buf, rp.logh, tw, logPmax, inv);
-        return;
+        if (rp.logh == 0) return buf;
+        return inv ? stockham<T, true>(buf, buf2, rp.logh, tw, logPmax, lt, tpf, g)
+                   : stockham<T, false>(buf, buf2, rp.logh, tw, logPmax, lt, tpf, g);
     }
-    // Bluestein; inverse via conj(DFT(conj z))
-    __syncthreads();
+    // Bluestein; inverse via conj(DFT(conj z)).  c_j = e^{-i pi j^2/h}.
     const int P = 1 << rp.logP;
-    const int h = rp.h, n = rp.nphi;
-    for (int j = threadIdx.x; j < P; j += blockDim.x) {
+    const int h = rp.h;
+    for (int j = lt; j < P; j += tpf) {
         cplx<T> a = {(T)0, (T)0};
         if (j < h) {
             a = buf[j];
             if (inv) a.im = -a.im;
-            // c_j = e^{-i pi j^2 / h} = E(2 j^2 mod 2n)
-            long long q = (2ll * j * j) % (2 * n);
-            a = cmul(a, E((int)q));
+            a = cmul(a, chirp[j]);
         }
         buf[j] = a;
     }
-    __syncthreads();
-    fft_dif(buf, rp.logP, tw, logPmax, false);
+    group_sync(tpf, g);
+    cplx<T>* r = stockham<T, false>(buf, buf2, rp.logP, tw, logPmax, lt, tpf, g);
+    cplx<T>* o = (r == buf) ? buf2 : buf;
     const cplx<T>* G = gtab + rp.gtab_off;
-    for (int j = threadIdx.x; j < P; j += blockDim.x) buf[j] = cmul(buf[j], G[j]);
-    __syncthreads();
-    fft_dit(buf, rp.logP, tw, logPmax, true);
-    for (int k = threadIdx.x; k < h; k += blockDim.x) {
-        long long q = (2ll * k * k) % (2 * n);
-        cplx<T> v = cmul(buf[k], E((int)q));
+    for (int j = lt; j < P; j += tpf) r[j] = cmul(r[j], G[j]);
+    group_sync(tpf, g);
+    r = stockham<T, true>(r, o, rp.logP, tw, logPmax, lt, tpf, g);
+    for (int k = lt; k < h; k += tpf) {
+        cplx<T> v = cmul(r[k], chirp[k]);
         if (inv) v.im = -v.im;
-        buf[k] = v;
+        r[k] = v;
     }
-    __syncthreads();
+    group_sync(tpf, g);
+    return r;
 }
 
+// Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
 template <typename T>
-__device__ __forceinline__ cplx<T> zget(const cplx<T>* buf, const RingPair& rp, int k) {
-    return rp.logh >= 0 ? buf[bitrev(k, rp.logh)] : buf[k];
-}
-
-// Forward transform of one real ring x[0..n) into F[0..mt).
-template <typename T>
-__device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* F, const RingPair& rp,
-                             const cplx<T>* __restrict__ tw, int logPmax, const cplx<T>* __restrict__ gtab,
-                             const PhaseTab<T>& E) {
+__device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ F,
+                             const RingPair& rp, const cplx<T>* __restrict__ tw, int logPmax,
+                             const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+                             const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h;
-    for (int j = threadIdx.x; j < h; j += blockDim.x) {
-        buf[j] = {x[2 * j], x[2 * j + 1]};
+    for (int j = lt; j < h; j += tpf) {
+        buf[j] = *(const cplx<T>*)(x + 2 * j);
     }
-    ring_dft(buf, rp, tw, logPmax, gtab, E, false);
-    for (int k = threadIdx.x; k < rp.mt; k += blockDim.x) {
-        int k1 = k == h ? 0 : k;
-        int k2 = k == 0 ? 0 : h - k;
-        cplx<T> Zk = zget(buf, rp, k1);
-        cplx<T> Zc = cconj(zget(buf, rp, k2));
-        cplx<T> Ek = cscale(cadd(Zk, Zc), (T)0.5);
-        cplx<T> d = cscale(csub(Zk, Zc), (T)0.5);
-        cplx<T> Ok = {d.im, -d.re};  // -i * d
+    cplx<T>* Z = ring_dft(buf, buf2, rp, tw, logPmax, gtab, chirp, false, lt, tpf, g);
+    for (int k = lt; k < rp.mt; k += tpf) {
+        const int k1 = k == h ? 0 : k;
+        const int k2 = k == 0 ? 0 : h - k;
+        const cplx<T> Zk = Z[k1];
+        const cplx<T> Zc = cconj(Z[k2]);
+        const cplx<T> Ek = cscale(cadd(Zk, Zc), (T)0.5);
+        const cplx<T> d = cscale(csub(Zk, Zc), (T)0.5);
+        const cplx<T> Ok = {d.im, -d.re};  // -i * d
         cplx<T> X = cadd(Ek, cmul(E(2 * k), Ok));
-        F[k] = cmul(E(shift * k), X);
+        if (shift) X = cmul(E(k), X);
+        *(cplx<T>*)(F + 2 * k) = X;
     }
+    group_sync(tpf, g);
 }
 
-// Inverse transform of spectrum F[0..mt) into one real ring x[0..n).
+// Inverse transform of spectrum Fs[0..mt) (shared memory) into one real ring x[0..n).
+// ref != nullptr: write ref - x (Jacobi residual).
 template <typename T>
-__device__ void ring_inverse(const cplx<T>* F, int shift, cplx<T>* buf, T* __restrict__ x, const RingPair& rp,
-                             const cplx<T>* __restrict__ tw, int logPmax, const cplx<T>* __restrict__ gtab,
-                             const PhaseTab<T>& E) {
+__device__ void ring_inverse(const cplx<T>* Fs, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ x,
+                             const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ tw,
+                             int logPmax, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+                             const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h, mt = rp.mt;
-    for (int k = threadIdx.x; k < h; k += blockDim.x) {
+    for (int k = lt; k < h; k += tpf) {
         // X_k and conj(X_{h-k}) with the phase e^{+i s k pi/n}; imag of X_0, X_h dropped
         cplx<T> Xa = {(T)0, (T)0}, Xb = {(T)0, (T)0};
-        if (k < mt) Xa = cmul(F[k], cconj(E(shift * k)));
-        int kb = h - k;
-        if (kb < mt) Xb = cconj(cmul(F[kb], cconj(E(shift * kb))));
+        if (k < mt) Xa = shift ? cmul(Fs[k], cconj(E(k))) : Fs[k];
+        const int kb = h - k;
+        if (kb < mt) Xb = cconj(shift ? cmul(Fs[kb], cconj(E(kb))) : Fs[kb]);
         if (k == 0) {
             Xa.im = (T)0;
             Xb.im = (T)0;
         }
-        cplx<T> sum = cadd(Xa, Xb), dif = csub(Xa, Xb);
-        cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
-        buf[k] = {sum.re - r.im, sum.im + r.re};   // sum + i r
+        const cplx<T> sum = cadd(Xa, Xb), dif = csub(Xa, Xb);
+        const cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
+        buf[k] = {sum.re - r.im, sum.im + r.re};       // sum + i r
     }
-    ring_dft(buf, rp, tw, logPmax, gtab, E, true);
-    for (int j = threadIdx.x; j < h; j += blockDim.x) {
-        cplx<T> z = zget(buf, rp, j);
-        x[2 * j] = z.re;
-        x[2 * j + 1] = z.im;
+    cplx<T>* z = ring_dft(buf, buf2, rp, tw, logPmax, gtab, chirp, true, lt, tpf, g);
+    for (int j = lt; j < h; j += tpf) {
+        cplx<T> v = z[j];
+        if (ref) {
+            const cplx<T> rv = *(const cplx<T>*)(ref + 2 * j);
+            v = csub(rv, v);
+        }
+        *(cplx<T>*)(x + 2 * j) = v;
     }
+    group_sync(tpf, g);
 }
 
 }  // namespace hpx
