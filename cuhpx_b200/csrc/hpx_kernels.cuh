@@ -7,8 +7,11 @@
 namespace hpx {
 
 // complex elements of dynamic shared memory the ring kernels need
+// (phase table, twiddles for P, and the padded work buffers of every FFT group:
+// groups x P <= 4096 whenever P <= 4096)
 __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
-    return 64 + (2 * (size_t)nmax + 63) / 64 + 2 * (size_t)(pfft_max > 4096 ? pfft_max : 4096);
+    return 64 + (2 * (size_t)nmax + 63) / 64 + (size_t)pfft_max / 2 +
+           2 * (size_t)padded_len(pfft_max > 4096 ? pfft_max : 4096) + 16;
 }
 
 // One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
@@ -25,14 +28,17 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
     const RingPair rp = pairs[south ? R - 1 - t : t];
     cplx<T>* elo = (cplx<T>*)smem_raw;
     cplx<T>* ehi = elo + 64;
-    cplx<T>* bufs = ehi + (2 * rp.nphi + 63) / 64;
+    cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
+    cplx<T>* bufs = twP + (1 << rp.logP) / 2;
     build_phase_tab(elo, ehi, rp.nphi);
+    if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
     __syncthreads();
     const PhaseTab<T> E{elo, ehi};
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
-    cplx<T>* buf = bufs + (size_t)g * 2 * P;
-    cplx<T>* buf2 = buf + P;
+    const int PL = padded_len(P);
+    cplx<T>* buf = bufs + (size_t)g * 2 * PL;
+    cplx<T>* buf2 = buf + PL;
     const int64_t start = south ? rp.start_s : rp.start_n;
     const int64_t foff = south ? rp.foff_s : rp.foff_n;
     const int shift = south ? rp.shift_s : rp.shift_n;
@@ -40,8 +46,8 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
     for (int b = b0 + g; b < b1; b += S)
-        ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff), rp, tw,
-                     logPmax, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+        ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff), rp, twP,
+                     gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
 }
 
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
@@ -59,14 +65,17 @@ __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64
     const RingPair rp = pairs[south ? R - 1 - t : t];
     cplx<T>* elo = (cplx<T>*)smem_raw;
     cplx<T>* ehi = elo + 64;
-    cplx<T>* bufs = ehi + (2 * rp.nphi + 63) / 64;
+    cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
+    cplx<T>* bufs = twP + (1 << rp.logP) / 2;
     build_phase_tab(elo, ehi, rp.nphi);
+    if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
     __syncthreads();
     const PhaseTab<T> E{elo, ehi};
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
-    cplx<T>* buf = bufs + (size_t)g * 2 * P;
-    cplx<T>* buf2 = buf + P;
+    const int PL = padded_len(P);
+    cplx<T>* buf = bufs + (size_t)g * 2 * PL;
+    cplx<T>* buf2 = buf + PL;
     const int64_t start = south ? rp.start_s : rp.start_n;
     const int64_t foff = south ? rp.foff_s : rp.foff_n;
     const int shift = south ? rp.shift_s : rp.shift_n;
@@ -75,8 +84,8 @@ __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64
     const int b1 = min(b0 + maps_per_cta, nmaps);
     for (int b = b0 + g; b < b1; b += S)
         ring_inverse((const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + foff)), shift, buf, buf2,
-                     map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr, rp, tw, logPmax,
-                     gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+                     map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr, rp, twP, gtab,
+                     chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
 }
 
 // Fold ring spectra into the m-major Legendre operand:
@@ -215,8 +224,10 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
     const RingPair rp = pairs[blockIdx.x];
     if (rp.logh >= 0) return;
     cplx<double>* buf = (cplx<double>*)smem_raw;
-    cplx<double>* buf2 = buf + (1 << rp.logP);
+    cplx<double>* buf2 = buf + padded_len(1 << rp.logP);
+    cplx<double>* twP = buf2 + padded_len(1 << rp.logP);
     const int P = 1 << rp.logP, h = rp.h;
+    load_twiddles(twP, rp.logP, tw64, logPmax);
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         const int d = j < h ? j : (j > P - h ? P - j : -1);
         cplx<double> v = {0.0, 0.0};
@@ -226,14 +237,14 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
             sincospi((double)q / (double)h, &s, &c);
             v = {c, s};
         }
-        buf[j] = v;
+        buf[padi(j)] = v;
         if (j < h) chirp[rp.gtab_off + j] = {(T)v.re, (T)(-v.im)};
     }
     __syncthreads();
-    cplx<double>* r = stockham<double, false>(buf, buf2, rp.logP, tw64, logPmax, threadIdx.x, blockDim.x, 0);
+    cplx<double>* r = stockham<double, false>(buf, buf2, rp.logP, twP, threadIdx.x, blockDim.x, 0);
     const double inv = 1.0 / (double)P;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
-        gtab[rp.gtab_off + j] = {(T)(r[j].re * inv), (T)(r[j].im * inv)};
+        gtab[rp.gtab_off + j] = {(T)(r[padi(j)].re * inv), (T)(r[padi(j)].im * inv)};
     }
 }
 

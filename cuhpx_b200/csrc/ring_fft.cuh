@@ -51,6 +51,11 @@ struct RingPair {
     double w;          // quadrature weight of the ring
 };
 
+// FFT work buffers are padded by one element every 16 so that the strided
+// Stockham stores of the first pass (stride 16 complex) spread over all banks.
+__device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int P) { return P + (P >> 4) + 1; }
+
 // ----------------------------------------------------------------- sync helpers
 // Threads [g*tpf, (g+1)*tpf) of the CTA form FFT group g.
 __device__ __forceinline__ void group_sync(int tpf, int g) {
@@ -63,79 +68,136 @@ __device__ __forceinline__ void group_sync(int tpf, int g) {
     }
 }
 
-// tw[q] = e^{-2 pi i q / Pmax} for q < Pmax/2; the other half by symmetry
-template <typename T>
-__device__ __forceinline__ cplx<T> twid(const cplx<T>* __restrict__ tw, int q, int half) {
-    if (q < half) return tw[q];
-    cplx<T> v = tw[q - half];
-    return {-v.re, -v.im};
+// 4-point DFT in registers (forward: e^-, inverse: e^+)
+template <typename T, bool INV>
+__device__ __forceinline__ void dft4(cplx<T>& v0, cplx<T>& v1, cplx<T>& v2, cplx<T>& v3) {
+    const cplx<T> t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
+    const cplx<T> d = csub(v1, v3);
+    const cplx<T> t3 = INV ? cplx<T>{-d.im, d.re} : cplx<T>{d.im, -d.re};  // +/- i d
+    v0 = cadd(t0, t2);
+    v1 = cadd(t1, t3);
+    v2 = csub(t0, t2);
+    v3 = csub(t1, t3);
 }
 
-// Stockham autosort radix-4/2 FFT of length P = 2^logP on src (natural order);
-// returns the buffer (src or dst) that holds the natural-order result.
-// INV: e^{+2 pi i jk/P} (unnormalised).  Threads: lt in [0, tpf) of group g.
+// 16-point DFT in registers as 4 x 4 with the internal factors W16^(b c).
 template <typename T, bool INV>
-__device__ cplx<T>* stockham(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ tw, int logPmax,
-                             int lt, int tpf, int g) {
+__device__ __forceinline__ void dft16(cplx<T>* v) {
+    // columns: v[b + 4a], a = 0..3
+#pragma unroll
+    for (int b = 0; b < 4; ++b) dft4<T, INV>(v[b], v[b + 4], v[b + 8], v[b + 12]);
+    // now v[b + 4c] = Y[b][c]; multiply by W16^(b c)
+    const T r = (T)0.70710678118654752440;  // cos(pi/4)
+    const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;  // cos/sin(pi/8)
+    const T sg = INV ? (T)1 : (T)-1;
+    // W16^k = cos(2 pi k/16) + sg*i sin(2 pi k/16)
+    const cplx<T> w1 = {c1, sg * s1}, w2 = {r, sg * r}, w3 = {s1, sg * c1}, w4 = {(T)0, sg},
+                  w6 = {-r, sg * r}, w9 = {-c1, -sg * s1};
+    v[1 + 4 * 1] = cmul(v[5], w1);
+    v[1 + 4 * 2] = cmul(v[9], w2);
+    v[1 + 4 * 3] = cmul(v[13], w3);
+    v[2 + 4 * 1] = cmul(v[6], w2);
+    v[2 + 4 * 2] = cmul(v[10], w4);
+    v[2 + 4 * 3] = cmul(v[14], w6);
+    v[3 + 4 * 1] = cmul(v[7], w3);
+    v[3 + 4 * 2] = cmul(v[11], w6);
+    v[3 + 4 * 3] = cmul(v[15], w9);
+    // rows: for each c, DFT over b -> X[c + 4d]
+#pragma unroll
+    for (int c = 0; c < 4; ++c) dft4<T, INV>(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+    // v[4c + d] = X[c + 4d]; reorder to natural order
+    cplx<T> o[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int d = 0; d < 4; ++d) o[c + 4 * d] = v[4 * c + d];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = o[i];
+}
+
+// Stockham autosort FFT of length P = 2^logP on src (natural order); returns the
+// buffer (src or dst) holding the natural-order result.  twP[q] = e^{-2 pi i q/P}
+// for q < P/2 (shared memory).  INV: e^{+2 pi i jk/P} (unnormalised).
+// First pass radix-16 in registers (contiguous 16-element stores), then radix-4
+// stages, and one radix-2 stage when log2(P) is odd.
+template <typename T, bool INV>
+__device__ cplx<T>* stockham(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt,
+                             int tpf, int g) {
     const int P = 1 << logP;
-    const int half = 1 << (logPmax - 1);
     int Ns = 1;
     int rem = logP;
-    while (rem > 0) {
-        if (rem >= 2) {
-            const int Q = P >> 2;
-            const int step = (1 << logPmax) / (Ns * 4);  // twiddle index stride
-            for (int j = lt; j < Q; j += tpf) {
-                const int k = j & (Ns - 1);
-                cplx<T> v0 = src[j], v1 = src[j + Q], v2 = src[j + 2 * Q], v3 = src[j + 3 * Q];
-                if (Ns > 1) {
-                    cplx<T> w1 = twid(tw, k * step, half), w2 = twid(tw, 2 * k * step, half),
-                            w3 = twid(tw, 3 * k * step, half);
-                    if (INV) {
-                        w1.im = -w1.im;
-                        w2.im = -w2.im;
-                        w3.im = -w3.im;
-                    }
-                    v1 = cmul(v1, w1);
-                    v2 = cmul(v2, w2);
-                    v3 = cmul(v3, w3);
-                }
-                const cplx<T> t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
-                const cplx<T> d = csub(v1, v3);
-                // forward: -i*d ; inverse: +i*d
-                const cplx<T> t3 = INV ? cplx<T>{-d.im, d.re} : cplx<T>{d.im, -d.re};
-                const int o = ((j - k) << 2) + k;
-                dst[o] = cadd(t0, t2);
-                dst[o + Ns] = cadd(t1, t3);
-                dst[o + 2 * Ns] = csub(t0, t2);
-                dst[o + 3 * Ns] = csub(t1, t3);
-            }
-            Ns <<= 2;
-            rem -= 2;
-        } else {
-            const int Q = P >> 1;
-            const int step = (1 << logPmax) / (Ns * 2);
-            for (int j = lt; j < Q; j += tpf) {
-                const int k = j & (Ns - 1);
-                cplx<T> v0 = src[j], v1 = src[j + Q];
-                if (Ns > 1) {
-                    cplx<T> w = twid(tw, k * step, half);
-                    if (INV) w.im = -w.im;
-                    v1 = cmul(v1, w);
-                }
-                const int o = ((j - k) << 1) + k;
-                dst[o] = cadd(v0, v1);
-                dst[o + Ns] = csub(v0, v1);
-            }
-            Ns <<= 1;
-            rem -= 1;
-        }
+    auto swap_bufs = [&]() {
         group_sync(tpf, g);
         cplx<T>* t = src;
         src = dst;
         dst = t;
+    };
+    if (rem >= 4) {
+        const int Q = P >> 4;
+        for (int j = lt; j < Q; j += tpf) {
+            cplx<T> v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = src[padi(j + r * Q)];
+            dft16<T, INV>(v);
+            // outputs 16j .. 16j+15 are one aligned 16-run: padded index 17j + r
+#pragma unroll
+            for (int r = 0; r < 16; ++r) dst[17 * j + r] = v[r];
+        }
+        Ns = 16;
+        rem -= 4;
+        swap_bufs();
+    }
+    while (rem >= 2) {
+        const int Q = P >> 2;
+        const int step = P / (Ns * 4);
+        for (int j = lt; j < Q; j += tpf) {
+            const int k = j & (Ns - 1);
+            cplx<T> v0 = src[padi(j)], v1 = src[padi(j + Q)], v2 = src[padi(j + 2 * Q)], v3 = src[padi(j + 3 * Q)];
+            if (Ns > 1) {
+                cplx<T> w1 = twP[k * step];
+                if (INV) w1.im = -w1.im;
+                const cplx<T> w2 = cmul(w1, w1), w3 = cmul(w1, w2);
+                v1 = cmul(v1, w1);
+                v2 = cmul(v2, w2);
+                v3 = cmul(v3, w3);
+            }
+            dft4<T, INV>(v0, v1, v2, v3);
+            const int o = ((j - k) << 2) + k;
+            dst[padi(o)] = v0;
+            dst[padi(o + Ns)] = v1;
+            dst[padi(o + 2 * Ns)] = v2;
+            dst[padi(o + 3 * Ns)] = v3;
+        }
+        Ns <<= 2;
+        rem -= 2;
+        swap_bufs();
+    }
+    if (rem == 1) {
+        const int Q = P >> 1;
+        const int step = P / (Ns * 2);
+        for (int j = lt; j < Q; j += tpf) {
+            const int k = j & (Ns - 1);
+            cplx<T> v0 = src[padi(j)], v1 = src[padi(j + Q)];
+            if (Ns > 1) {
+                cplx<T> w = twP[k * step];
+                if (INV) w.im = -w.im;
+                v1 = cmul(v1, w);
+            }
+            const int o = ((j - k) << 1) + k;
+            dst[padi(o)] = cadd(v0, v1);
+            dst[padi(o + Ns)] = csub(v0, v1);
+        }
+        swap_bufs();
     }
     return src;
+}
+
+// twP[q] = e^{-2 pi i q / P}, q < P/2, from the plan's table for Pmax (all threads of the CTA)
+template <typename T>
+__device__ void load_twiddles(cplx<T>* twP, int logP, const cplx<T>* __restrict__ tw, int logPmax) {
+    const int half = 1 << (logP - 1);
+    const int stride = 1 << (logPmax - logP);
+    for (int q = threadIdx.x; q < half; q += blockDim.x) twP[q] = tw[q * stride];
 }
 
 // e^{-i pi q / n} for 0 <= q < 2n from two small tables: q = 64*hi + lo
@@ -161,14 +223,14 @@ __device__ void build_phase_tab(cplx<T>* lo, cplx<T>* hi, int n) {
 // Complex DFT of length h of buf (natural order, h entries written by this
 // group), forward (e^-) or inverse (e^+); returns the buffer with Z in natural order.
 template <typename T>
-__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const cplx<T>* __restrict__ tw,
-                             int logPmax, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
-                             bool inv, int lt, int tpf, int g) {
+__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const cplx<T>* __restrict__ twP,
+                             const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp, bool inv, int lt,
+                             int tpf, int g) {
     group_sync(tpf, g);
     if (rp.logh >= 0) {
         if (rp.logh == 0) return buf;
-        return inv ? stockham<T, true>(buf, buf2, rp.logh, tw, logPmax, lt, tpf, g)
-                   : stockham<T, false>(buf, buf2, rp.logh, tw, logPmax, lt, tpf, g);
+        return inv ? stockham<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g)
+                   : stockham<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g);
     }
     // Bluestein; inverse via conj(DFT(conj z)).  c_j = e^{-i pi j^2/h}.
     const int P = 1 << rp.logP;
@@ -176,23 +238,23 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
     for (int j = lt; j < P; j += tpf) {
         cplx<T> a = {(T)0, (T)0};
         if (j < h) {
-            a = buf[j];
+            a = buf[padi(j)];
             if (inv) a.im = -a.im;
             a = cmul(a, chirp[j]);
         }
-        buf[j] = a;
+        buf[padi(j)] = a;
     }
     group_sync(tpf, g);
-    cplx<T>* r = stockham<T, false>(buf, buf2, rp.logP, tw, logPmax, lt, tpf, g);
+    cplx<T>* r = stockham<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g);
     cplx<T>* o = (r == buf) ? buf2 : buf;
     const cplx<T>* G = gtab + rp.gtab_off;
-    for (int j = lt; j < P; j += tpf) r[j] = cmul(r[j], G[j]);
+    for (int j = lt; j < P; j += tpf) r[padi(j)] = cmul(r[padi(j)], G[j]);
     group_sync(tpf, g);
-    r = stockham<T, true>(r, o, rp.logP, tw, logPmax, lt, tpf, g);
+    r = stockham<T, true>(r, o, rp.logP, twP, lt, tpf, g);
     for (int k = lt; k < h; k += tpf) {
-        cplx<T> v = cmul(r[k], chirp[k]);
+        cplx<T> v = cmul(r[padi(k)], chirp[k]);
         if (inv) v.im = -v.im;
-        r[k] = v;
+        r[padi(k)] = v;
     }
     group_sync(tpf, g);
     return r;
@@ -201,19 +263,18 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
 // Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
 template <typename T>
 __device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ F,
-                             const RingPair& rp, const cplx<T>* __restrict__ tw, int logPmax,
-                             const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
-                             const PhaseTab<T>& E, int lt, int tpf, int g) {
+                             const RingPair& rp, const cplx<T>* __restrict__ twP, const cplx<T>* __restrict__ gtab,
+                             const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h;
     for (int j = lt; j < h; j += tpf) {
-        buf[j] = *(const cplx<T>*)(x + 2 * j);
+        buf[padi(j)] = *(const cplx<T>*)(x + 2 * j);
     }
-    cplx<T>* Z = ring_dft(buf, buf2, rp, tw, logPmax, gtab, chirp, false, lt, tpf, g);
+    cplx<T>* Z = ring_dft(buf, buf2, rp, twP, gtab, chirp, false, lt, tpf, g);
     for (int k = lt; k < rp.mt; k += tpf) {
         const int k1 = k == h ? 0 : k;
         const int k2 = k == 0 ? 0 : h - k;
-        const cplx<T> Zk = Z[k1];
-        const cplx<T> Zc = cconj(Z[k2]);
+        const cplx<T> Zk = Z[padi(k1)];
+        const cplx<T> Zc = cconj(Z[padi(k2)]);
         const cplx<T> Ek = cscale(cadd(Zk, Zc), (T)0.5);
         const cplx<T> d = cscale(csub(Zk, Zc), (T)0.5);
         const cplx<T> Ok = {d.im, -d.re};  // -i * d
@@ -228,8 +289,8 @@ __device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, c
 // ref != nullptr: write ref - x (Jacobi residual).
 template <typename T>
 __device__ void ring_inverse(const cplx<T>* Fs, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ x,
-                             const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ tw,
-                             int logPmax, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+                             const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ twP,
+                             const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
                              const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h, mt = rp.mt;
     for (int k = lt; k < h; k += tpf) {
@@ -244,11 +305,11 @@ __device__ void ring_inverse(const cplx<T>* Fs, int shift, cplx<T>* buf, cplx<T>
         }
         const cplx<T> sum = cadd(Xa, Xb), dif = csub(Xa, Xb);
         const cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
-        buf[k] = {sum.re - r.im, sum.im + r.re};       // sum + i r
+        buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
     }
-    cplx<T>* z = ring_dft(buf, buf2, rp, tw, logPmax, gtab, chirp, true, lt, tpf, g);
+    cplx<T>* z = ring_dft(buf, buf2, rp, twP, gtab, chirp, true, lt, tpf, g);
     for (int j = lt; j < h; j += tpf) {
-        cplx<T> v = z[j];
+        cplx<T> v = z[padi(j)];
         if (ref) {
             const cplx<T> rv = *(const cplx<T>*)(ref + 2 * j);
             v = csub(rv, v);
