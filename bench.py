@@ -270,6 +270,15 @@ def run_gpu(args):
     clk = clocks.stop()
     stats = plan.stats_read()
     plan.stats_enable(False)
+    plan.check()  # raises if a tensor-core pipeline wait gave up during the timed steps
+    # the timed result must be a real transform: compare one batch with the plain FP32 path
+    with torch.no_grad():
+        ref = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision="fp32")(f[:4])
+        got = sht(f[:4])
+        plan.check()
+        check_rel = float((got - ref).abs().pow(2).sum().sqrt() / ref.abs().pow(2).sum().sqrt())
+    if not (check_rel < 1e-3):
+        raise RuntimeError(f"timed transform disagrees with the FP32 path: rel-L2 {check_rel:.3e}")
     ms_step = ms / args.steps
     value = world * B * args.steps / (ms / 1000.0)
     launches_per_step = sum(v[0] for v in stats.values()) / args.steps
@@ -344,6 +353,7 @@ def run_gpu(args):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "plain_fp32_maps_per_s": plain,
+            "check_rel_l2_vs_fp32": check_rel,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

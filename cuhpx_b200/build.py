@@ -42,8 +42,10 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
-def build(force=False, debug=False, verbose=False):
-    if not force and up_to_date():
+def build(force=False, debug=False, verbose=False, defines=(), out=None):
+    """Compile the library; ``defines``/``out`` build an instrumented copy elsewhere."""
+    target = out or LIB
+    if not force and out is None and not defines and up_to_date():
         return LIB
     cmd = [
         _nvcc(),
@@ -60,19 +62,21 @@ def build(force=False, debug=False, verbose=False):
         "-I",
         os.path.join(REPO, "include"),
         "-o",
-        LIB + ".tmp",
+        target + ".tmp",
         *[os.path.join(CSRC, s) for s in SOURCES],
     ]
     if debug:
         cmd.insert(1, "-DHPX_CHECK_BOUNDS=1")
+    for d in defines:
+        cmd.insert(1, "-D" + d)
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc failed building libhpx_b200.so")
     if verbose:
         sys.stderr.write(res.stderr)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(target + ".tmp", target)
+    return target
 
 
 if __name__ == "__main__":
@@ -80,5 +84,7 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--debug", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[])
+    ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    print(build(force=a.force, debug=a.debug, verbose=a.verbose))
+    print(build(force=a.force or bool(a.out), debug=a.debug, verbose=a.verbose, defines=a.defines, out=a.out))

@@ -99,6 +99,9 @@ struct hpx_plan_s {
     double2* d_coef = nullptr;   // [M][Lpad] recurrence coefficients
     double2* d_seeds = nullptr;  // [M][seed_blocks(L)][2*nside] block seeds
     int2* d_fwdtiles = nullptr;  // (m, degree block) tiles of the forward contraction
+    double* d_z = nullptr;       // cos(theta) of the north rings
+    AlphaC* d_alphac = nullptr;  // [M][Lpad] block-normalised recurrence (tensor-core producers)
+    int* d_lsmax = nullptr;      // per order: max over its rings of the first significant degree
     int n_fwdtiles = 0;
     size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
@@ -140,6 +143,9 @@ struct hpx_plan_s {
         cudaFree(d_coef);
         cudaFree(d_seeds);
         cudaFree(d_fwdtiles);
+        cudaFree(d_z);
+        cudaFree(d_alphac);
+        cudaFree(d_lsmax);
         cudaFree(tc.d_err);
         cudaFree(tc.d_fwd_tiles);
         cudaFree(tc.d_inv_tiles);
@@ -259,17 +265,17 @@ int tc_create(hpx_plan_s* P) {
         HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * it.size()));
         HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
     }
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
     T.active = 1;
     return HPX_OK;
 }
 
-// 3-D bf16 tensor map over [outer][rows][128 cols] with a {64 cols, 32 rows} box, 128B swizzle.
-int encode_operand(const hpx_plan_s* P, CUtensorMap* map, void* base, uint64_t rows, uint64_t outer) {
+// 3-D bf16 tensor map over [outer][rows][128 cols] with a {64 cols, box_rows} box, 128B swizzle.
+int encode_operand(const hpx_plan_s* P, CUtensorMap* map, void* base, uint64_t rows, uint64_t outer, int box_rows) {
     const cuuint64_t dims[3] = {(cuuint64_t)kTcCols, rows, outer};
     const cuuint64_t strides[2] = {(cuuint64_t)kTcCols * 2, (cuuint64_t)kTcCols * 2 * rows};
-    const cuuint32_t box[3] = {64, 32, 1};
+    const cuuint32_t box[3] = {64, (cuuint32_t)box_rows, 1};
     const cuuint32_t es[3] = {1, 1, 1};
     CUresult r = ((EncodeTiledFn)P->tc.encode)(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, es,
                                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -378,12 +384,37 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     if (e != cudaSuccess || e2 != cudaSuccess)
         return set_err(HPX_ERR_CUDA, std::string("legendre start: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
 
+    // ---- compact ring z and per-order max start degree (fast-path test of the tensor-core producers)
+    {
+        std::vector<double> hz(P->NP);
+        for (int p = 0; p < P->NP; ++p) hz[p] = P->h_pairs[p].z;
+        HPX_CUDA_TRY(cudaMalloc(&P->d_z, sizeof(double) * P->NP));
+        HPX_CUDA_TRY(cudaMemcpy(P->d_z, hz.data(), sizeof(double) * P->NP, cudaMemcpyHostToDevice));
+        std::vector<int> hls((size_t)nms), hmax(P->M, 0);
+        HPX_CUDA_TRY(cudaMemcpy(hls.data(), P->d_lstart, sizeof(int) * nms, cudaMemcpyDeviceToHost));
+        for (int m = 0; m < P->M; ++m) {
+            const int t0 = first_ring_for_m(m, N);
+            int mx = m;
+            for (int p = t0; p < P->NP; ++p) mx = std::max(mx, hls[(size_t)m * P->NP + p]);
+            hmax[m] = mx;
+        }
+        HPX_CUDA_TRY(cudaMalloc(&P->d_lsmax, sizeof(int) * P->M));
+        HPX_CUDA_TRY(cudaMemcpy(P->d_lsmax, hmax.data(), sizeof(int) * P->M, cudaMemcpyHostToDevice));
+    }
+
     // ---- recurrence coefficients and degree-block seeds (FP64)
     P->Lpad = P->L + kCoefPad;
     HPX_CUDA_TRY(cudaMalloc(&P->d_coef, sizeof(double2) * (size_t)P->M * P->Lpad));
     {
         const int64_t n = (int64_t)P->M * P->Lpad;
         k_legendre_coef<<<(unsigned)((n + 255) / 256), 256>>>(P->M, P->L, P->Lpad, P->d_coef);
+        HPX_CUDA_TRY(cudaGetLastError());
+    }
+    HPX_CUDA_TRY(cudaMalloc(&P->d_alphac, sizeof(AlphaC) * (size_t)P->M * P->Lpad));
+    HPX_CUDA_TRY(cudaMemset(P->d_alphac, 0, sizeof(AlphaC) * (size_t)P->M * P->Lpad));
+    {
+        const int64_t n = (int64_t)P->M * seed_blocks(P->L);
+        k_legendre_alpha<<<(unsigned)((n + 127) / 128), 128>>>(P->M, P->L, P->Lpad, P->d_coef, P->d_alphac);
         HPX_CUDA_TRY(cudaGetLastError());
     }
     const size_t nseed = (size_t)P->M * seed_blocks(P->L) * P->NP;
@@ -534,11 +565,11 @@ struct Pipeline {
                 k_zero_alm_cols<<<1024, 256, 0, st>>>((float*)alm, nb, P->L, P->M, TP.m_tc_end);
             if (TP.n_fwd_tiles == 0) return;
             CUtensorMap mh, ml;
-            if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M)) != HPX_OK) return;
-            if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M)) != HPX_OK) return;
-            k_leg_fwd_tc<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kTcSmem, st>>>(
-                mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_pairs, P->d_lstart, P->d_pstart,
-                P->d_coef, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, TP.d_err);
+            if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
+            if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
+            k_leg_fwd_tc<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kFSmem, st>>>(
+                mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, TP.d_err);
             return;
         }
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
@@ -564,11 +595,11 @@ struct Pipeline {
                                 (size_t)(P->M - TP.m_tc_end) * 2 * P->NP * C * sizeof(T), st);
             if (TP.n_inv_tiles == 0) return;
             CUtensorMap mh, ml;
-            if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M)) != HPX_OK) return;
-            if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M)) != HPX_OK) return;
-            k_leg_inv_tc<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kTcSmem, st>>>(
-                mh, ml, (float*)spec, C, P->L, P->M, P->Lpad, P->nside, P->d_pairs, P->d_lstart, P->d_pstart,
-                P->d_coef, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, TP.d_err);
+            if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
+            if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
+            k_leg_inv_tc<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kISmem, st>>>(
+                mh, ml, (float*)spec, C, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, TP.d_err);
             return;
         }
         dim3 tg((P->M + 31) / 32, P->L, (nb + 15) / 16);
@@ -807,6 +838,16 @@ const char* hpx_status_string(int status) {
         default: return "unknown status";
     }
 }
+
+#ifdef HPX_TC_PROFILE
+// Instrumented builds only: copy and clear the per-CTA role timers.
+extern "C" HPX_API int hpx_tc_profile_read(unsigned long long* out) {
+    cudaMemcpyFromSymbol(out, g_tc_prof, sizeof(g_tc_prof));
+    static unsigned long long zero[2][296][8];
+    cudaMemcpyToSymbol(g_tc_prof, zero, sizeof(g_tc_prof));
+    return HPX_OK;
+}
+#endif
 
 const char* hpx_version(void) { return "hpx_b200 0.1.0 (sm_100a)"; }
 

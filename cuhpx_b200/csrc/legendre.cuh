@@ -35,7 +35,8 @@ __device__ __forceinline__ double rec_b(int l, int m) {
     return sqrt((dl + dm - 1.0) / (dl - dm) * (2.0 * dl + 1.0) / (2.0 * dl - 3.0) * (dl - dm - 1.0) / (dl + dm));
 }
 
-constexpr double kSeedLog2Floor = -600.0;
+// Values below 2^-1000 (still normal doubles) are treated as zero.
+constexpr double kSeedLog2Floor = -1000.0;
 
 // Start values of the recurrence for (m, north ring p); see file comment.
 // logc[m] = log2(Pbar_m^m / sin^m(theta)) = log2(1/sqrt(4pi)) + 0.5 sum_k log2((2k+1)/(2k)).
@@ -69,10 +70,10 @@ __global__ void k_legendre_start(int M, int L, int nside, const RingPair* __rest
             q1 = q2;
             ++l;
             double mx = fmax(fabs(q0), fabs(q1));
-            if (mx > 0x1p500) {
-                q0 = ldexp(q0, -500);
-                q1 = ldexp(q1, -500);
-                E += 500.0;
+            if (mx > 0x1p400) {
+                q0 = ldexp(q0, -400);
+                q1 = ldexp(q1, -400);
+                E += 400.0;
             }
         }
     }
@@ -133,6 +134,50 @@ __global__ void k_legendre_seeds(int M, int L, int Lpad, int nside, const RingPa
         else if (off == 1) out[(int64_t)j * NP].y = v;
         p2 = p1;
         p1 = v;
+    }
+}
+
+// Block-normalised recurrence used by the tensor-core producers.  Inside the
+// 64-degree block that starts at l0b (seed pair P_{l0b}, P_{l0b+1}) write
+// P_l = c_l q_l with c_{l0b} = c_{l0b+1} = 1 and c_l = b_l c_{l-2}; then
+//   q_l = alpha_l x q_{l-1} - q_{l-2},   alpha_l = a_l c_{l-1} / c_l,
+// so each step is one FP64 multiply off the dependency chain plus one FMA on
+// it, and the scale c_l is applied after rounding to FP32.
+struct __align__(16) AlphaC {
+    double alpha;
+    float c;
+    float pad;
+};
+
+__global__ void k_legendre_alpha(int M, int L, int Lpad, const double2* __restrict__ coef, AlphaC* __restrict__ out) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // one thread per (m, block)
+    const int nb = seed_blocks(L);
+    if (idx >= (int64_t)M * nb) return;
+    const int m = (int)(idx / nb), j = (int)(idx % nb);
+    const int l0b = m + j * kSeedBlock;
+    AlphaC* o = out + (int64_t)m * Lpad;
+    if (l0b >= L && j > 0) return;
+    double cm2 = 1.0, cm1 = 1.0;  // c_{l-2}, c_{l-1}
+    for (int i = 0; i < kSeedBlock; ++i) {
+        const int l = l0b + i;
+        if (l >= Lpad) break;
+        AlphaC v;
+        v.pad = 0.f;
+        if (i < 2 || l >= L || l < m + 2) {
+            v.alpha = 0.0;
+            v.c = (l < L && i < 2) ? 1.f : 0.f;
+            const double c = (i < 2) ? 1.0 : 0.0;
+            cm2 = cm1;
+            cm1 = c;
+        } else {
+            const double2 ab = coef[(int64_t)m * Lpad + l];
+            const double c = ab.y * cm2;
+            v.alpha = ab.x * cm1 / c;
+            v.c = (float)c;
+            cm2 = cm1;
+            cm1 = c;
+        }
+        o[l] = v;
     }
 }
 
@@ -363,7 +408,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
     const int tid = threadIdx.x;
     double* coefA = (double*)smem_raw;
     double* coefB = coefA + L;
-    T* Pt = (T*)(((uintptr_t)(coefB + L) + 15) & ~(uintptr_t)15);  // [LC][RBP]
+    T* Pt = (T*)(coefB + L);  // [LC][RBP], 16-byte aligned (2L doubles precede it)
     T* As = Pt + LC * RBP;                                          // [LC][CT]
 
     const int t0 = first_ring_for_m(m, nside);

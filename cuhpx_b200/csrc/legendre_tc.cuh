@@ -34,15 +34,33 @@
 
 namespace hpx {
 
+// Optional per-CTA role timers (built only with -DHPX_TC_PROFILE): cycles each
+// role spends waiting vs working, read back by hpx_tc_profile_read.
+#ifdef HPX_TC_PROFILE
+__device__ unsigned long long g_tc_prof[2][148 * 2][8];
+#define TCP_T0(v) long long v = clock64()
+#define TCP_ADD(k, slot, v) atomicAdd(&g_tc_prof[k][blockIdx.x % 296][slot], (unsigned long long)(clock64() - (v)))
+#else
+#define TCP_T0(v)
+#define TCP_ADD(k, slot, v)
+#endif
+
 constexpr int kTcCols = 128;      // N: columns per tile (64 maps)
-constexpr int kTcStages = 3;      // smem pipeline depth
-constexpr int kTcRingChunk = 32;  // K per analysis stage (rings)
+constexpr int kTcThreads = 512;   // 16 warps
+// analysis: 6 stages of 16 rings (32 KB: A 4 x 4 KB, B 4 x 4 KB)
+constexpr int kFStages = 6;
+constexpr int kFRing = 16;
+constexpr int kFStageBytes = 32768;
 constexpr int kTcFwdDeg = 256;    // degrees per analysis tile (128 per parity)
+constexpr int kFCoef = 256;       // per-producer-warp coefficient window (AlphaC)
+constexpr int kFSmem = kFStages * kFStageBytes + 8 * kFCoef * 16 + 1024 + 1024;
+// synthesis: 3 stages of 64 degrees (64 KB: A 4 x 8 KB, B 4 x 8 KB)
+constexpr int kIStages = 3;
+constexpr int kIStageBytes = 65536;
 constexpr int kTcInvRings = 128;  // rings per synthesis tile
 constexpr int kTcDegChunk = 64;   // degrees per synthesis stage (32 per parity)
-constexpr int kTcThreads = 512;   // 16 warps
-constexpr int kTcStageBytes = 65536;
-constexpr int kTcSmem = kTcStages * kTcStageBytes + 8 * 1024 + 1024 + 1024;
+constexpr int kISmem = kIStages * kIStageBytes + 8 * 64 * 16 + 1024 + 1024;
+constexpr int kMaxStages = 6;
 
 // Host-side state of the tensor-core path, owned by the plan.
 struct TcPlan {
@@ -60,9 +78,9 @@ struct TcPlan {
 
 // ------------------------------------------------------------------ shared layout
 struct TcShared {
-    uint64_t full_tma[kTcStages];
-    uint64_t full_prod[kTcStages];
-    uint64_t empty[kTcStages];
+    uint64_t full_tma[kMaxStages];
+    uint64_t full_prod[kMaxStages];
+    uint64_t empty[kMaxStages];
     uint64_t acc_full[2];
     uint64_t acc_empty[2];
     uint64_t drain;
@@ -71,33 +89,20 @@ struct TcShared {
 
 __device__ __forceinline__ uint32_t pack_bf16x2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
 
-// split 8 doubles into bf16 hi/lo 16-byte vectors
-__device__ __forceinline__ void split8(const double* v, uint4& hi, uint4& lo) {
-    uint16_t h[8], l[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) tc::split_bf16((float)v[i], h[i], l[i]);
-    hi = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]), pack_bf16x2(h[4], h[5]), pack_bf16x2(h[6], h[7]));
-    lo = make_uint4(pack_bf16x2(l[0], l[1]), pack_bf16x2(l[2], l[3]), pack_bf16x2(l[4], l[5]), pack_bf16x2(l[6], l[7]));
+// x ~ hi + lo for two floats: hi = bf16_rn(x), lo = bf16_rn(x - hi) (packed conversions)
+__device__ __forceinline__ uint32_t split_pair(float fa, float fb, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(fa, fb);
+    const uint32_t hb = *(const uint32_t*)&h;
+    const float ha = __uint_as_float(hb << 16), hbf = __uint_as_float(hb & 0xffff0000u);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(fa - ha, fb - hbf);
+    lo = *(const uint32_t*)&l;
+    return hb;
 }
-
-// On exit (normal or after a timeout) the TMA thread waits, bounded, for the
-// loads it issued into the last pipeline stages, so no bulk copy lands in
-// shared memory after the CTA has finished.
-__device__ __forceinline__ void tma_drain(TcShared* sh, int issued, int* err) {
-    (void)err;
-    for (int k = 1; k <= kTcStages && issued - k >= 0; ++k) {
-        const int it = issued - k;
-        int local = 0;  // bounded wait that does not stop early on another role's error
-        tc::mbar_wait(&sh->full_tma[it % kTcStages], (it / kTcStages) & 1, &local, 0);
-    }
-}
-// The MMA thread commits once more and waits, bounded, so that every MMA it
-// issued has retired before TMEM is released.
-__device__ __forceinline__ void mma_drain(TcShared* sh, int* err) {
-    tc::mma_commit(&sh->drain);
-    int dummy = 0;
-    tc::mbar_wait(&sh->drain, 0, &dummy, 0);
-    (void)err;
+__device__ __forceinline__ void split8f(const float* v, uint4& hi, uint4& lo) {
+    hi.x = split_pair(v[0], v[1], lo.x);
+    hi.y = split_pair(v[2], v[3], lo.y);
+    hi.z = split_pair(v[4], v[5], lo.z);
+    hi.w = split_pair(v[6], v[7], lo.w);
 }
 
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
@@ -105,72 +110,27 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
                  : "memory");
 }
 
-// Generate 64 consecutive degrees l0b..l0b+63 of one ring from its block seed,
-// handing every 16 degrees (8 of each parity) to `emit(s, even8, odd8)`.
-template <typename Emit>
-__device__ __forceinline__ void gen_block64(int l0b, int L, int ls, double2 ps, double2 sd, double x,
-                                            const double2* __restrict__ cf, bool fast, Emit&& emit) {
-    double p2 = 0.0, p1 = 0.0;
-    double ev[8], od[8];
-    if (fast) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int i = s * 16 + k;
-                double v;
-                if (i == 0) v = sd.x;
-                else if (i == 1) v = sd.y;
-                else {
-                    const double2 ab = cf[i];
-                    v = ab.x * x * p1 - ab.y * p2;
-                }
-                p2 = p1;
-                p1 = v;
-                if (k & 1) od[k >> 1] = v; else ev[k >> 1] = v;
-            }
-            emit(s, ev, od);
-        }
-    } else {
-#pragma unroll 1
-        for (int s = 0; s < 4; ++s) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const int i = s * 16 + k;
-                const int l = l0b + i;
-                const double2 ab = cf[i];
-                double v = (l < L) ? leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2) : 0.0;
-                p2 = p1;
-                p1 = v;
-                if (k & 1) od[k >> 1] = v; else ev[k >> 1] = v;
-            }
-            emit(s, ev, od);
-        }
+// On exit (normal or after a timeout) the TMA thread waits, bounded, for the
+// loads it issued into the last pipeline stages, so no bulk copy lands in
+// shared memory after the CTA has finished.
+__device__ __forceinline__ void tma_drain(TcShared* sh, int issued, int stages) {
+    for (int k = 1; k <= stages && issued - k >= 0; ++k) {
+        const int it = issued - k;
+        tc::mbar_wait_quiet(&sh->full_tma[it % stages], (it / stages) & 1);
     }
 }
+// The MMA thread commits once more and waits, bounded, so that every MMA it
+// issued has retired before TMEM is released.
+__device__ __forceinline__ void mma_drain(TcShared* sh) {
+    tc::mma_commit(&sh->drain);
+    tc::mbar_wait_quiet(&sh->drain, 0);
+}
 
-// ================================================================== analysis
-// Xh/Xl: bf16 [2M][NP][128] (hi and lo of S (par 0) and D (par 1)) via tensor maps.
-__global__ void __launch_bounds__(kTcThreads, 1)
-    k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map, int nmaps,
-                 float* __restrict__ alm, int L, int M, int Lpad, int nside, const RingPair* __restrict__ pairs,
-                 const int* __restrict__ lstart, const double2* __restrict__ pstart, const double2* __restrict__ coef,
-                 const double2* __restrict__ seeds, const int2* __restrict__ tiles, int ntiles, int accumulate,
-                 int* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char* stages = base;                                           // kTcStages x 64 KB
-    double2* coef_s = (double2*)(base + kTcStages * kTcStageBytes);         // 8 producer warps x 64
-    TcShared* sh = (TcShared*)(base + kTcStages * kTcStageBytes + 8 * 1024);
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NP = 2 * nside;
-    const int nbk = seed_blocks(L);
-
-    if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
+__device__ __forceinline__ void tc_setup(TcShared* sh, int stages, int prod_arrivals, int warp) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) {
             tc::mbar_init(&sh->full_tma[s], 1);
-            tc::mbar_init(&sh->full_prod[s], 4);
+            tc::mbar_init(&sh->full_prod[s], prod_arrivals);
             tc::mbar_init(&sh->empty[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
@@ -187,10 +147,110 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
+}
+
+// Two independent block-normalised recurrences (64 degrees each) from their
+// seeds, interleaved for latency hiding.  Every 16 degrees, emit(chain, s,
+// even8, odd8) receives the FP32 values Pbar = c * q of 8 even and 8 odd degrees.
+template <typename Emit>
+__device__ __forceinline__ void gen2_fast(double2 sa, double2 sb, double xa, double xb, const AlphaC* __restrict__ ca,
+                                          const AlphaC* __restrict__ cb, Emit&& emit) {
+    double qa2 = 0.0, qa1 = 0.0, qb2 = 0.0, qb1 = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        float ea[8], oa[8], eb[8], ob[8];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int i = s * 16 + k;
+            const AlphaC A = ca[i];
+            const AlphaC B = cb[i];
+            double va, vb;
+            if (i == 0) {
+                va = sa.x;
+                vb = sb.x;
+            } else if (i == 1) {
+                va = sa.y;
+                vb = sb.y;
+            } else {
+                va = fma(A.alpha * xa, qa1, -qa2);
+                vb = fma(B.alpha * xb, qb1, -qb2);
+            }
+            qa2 = qa1;
+            qa1 = va;
+            qb2 = qb1;
+            qb1 = vb;
+            const float fa = (float)va * A.c, fb = (float)vb * B.c;
+            if (k & 1) {
+                oa[k >> 1] = fa;
+                ob[k >> 1] = fb;
+            } else {
+                ea[k >> 1] = fa;
+                eb[k >> 1] = fb;
+            }
+        }
+        emit(0, s, ea, oa);
+        emit(1, s, eb, ob);
+    }
+}
+
+// Reference-form recurrence with the l_s injection (orders whose first
+// significant degree lies inside this block; rare), coefficients from global memory.
+template <typename Emit>
+__device__ __forceinline__ void gen1_slow(int chain, int m, int l0b, int L, int Lpad, int ls, double2 ps, double2 sd,
+                                          double x, const double2* __restrict__ coef, Emit&& emit) {
+    double p2 = 0.0, p1 = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        float ev[8], od[8];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int i = s * 16 + k;
+            const int l = l0b + i;
+            double v;
+            if (i == 0 && ls <= l0b) v = sd.x;
+            else if (i == 1 && ls <= l0b) v = sd.y;
+            else {
+                const double2 ab = l < L && l >= m + 2 ? coef[(int64_t)m * Lpad + l] : make_double2(0.0, 0.0);
+                v = (l < L) ? leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2) : 0.0;
+            }
+            p2 = p1;
+            p1 = v;
+            if (k & 1) od[k >> 1] = (float)v; else ev[k >> 1] = (float)v;
+        }
+        emit(chain, s, ev, od);
+    }
+}
+
+// ================================================================== analysis
+// Xh/Xl: bf16 [2M][NP][128] (hi and lo of S (par 0) and D (par 1)) via tensor maps.
+// Tile (m, 256 degrees); pipeline chunk = 16 rings.  Stage layout:
+//   A_par,hl (Pbar, MN-major SW128, 128 l x 16 rings, 4 KB) at (par*2+hl)*4096
+//   B_par,hl (X,    MN-major SW128, 16 rings x 128 cols, 4 KB) at 16384 + (par*2+hl)*4096
+// Producer warp w < 6 owns pipeline stage w and takes the chunks it = w (mod 6):
+// a producer never runs more than one barrier phase ahead of the MMAs (with more
+// producer groups than stages an mbarrier parity wait could pass on a stale
+// phase).  Lane = (ring r = lane&15, block pair bp = lane>>4) runs the two
+// blocks 2bp, 2bp+1 of its ring.
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map, int nmaps,
+                 float* __restrict__ alm, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
+                 const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
+                 const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
+                 const int2* __restrict__ tiles, int ntiles, int accumulate, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // align by pointer arithmetic on the shared array (keeps the shared address space known)
+    unsigned char* base = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
+    unsigned char* stages = base;
+    AlphaC* coef_s = (AlphaC*)(base + kFStages * kFStageBytes);
+    TcShared* sh = (TcShared*)(base + kFStages * kFStageBytes + 8 * kFCoef * 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int NP = 2 * nside;
+    const int nbk = seed_blocks(L);
+    tc_setup(sh, kFStages, 1, warp);
     const uint32_t tmem = sh->tmem_base;
+    auto nchunks = [&](int m) { return (NP - first_ring_for_m(m, nside) + kFRing - 1) / kFRing; };
 
     if (warp == 0) {
-        // ------------------------------------------------ TMA producer
         if (lane == 0) {
             tc::tma_prefetch_desc(&xh_map);
             tc::tma_prefetch_desc(&xl_map);
@@ -198,68 +258,69 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
                 const int m = tiles[t].x;
                 const int t0 = first_ring_for_m(m, nside);
-                const int nch = (NP - t0 + kTcRingChunk - 1) / kTcRingChunk;
+                const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kTcStages;
-                    if (!tc::mbar_wait(&sh->empty[s], ((it / kTcStages) & 1) ^ 1, err, 11)) goto tma_done;
-                    unsigned char* st = stages + s * kTcStageBytes + 32768;  // B region
-                    tc::mbar_arrive_tx(&sh->full_tma[s], 32768);
-                    const int y = t0 + c * kTcRingChunk;
+                    const int s = it % kFStages;
+                    if (!tc::mbar_wait(&sh->empty[s], ((it / kFStages) & 1) ^ 1, err, 11)) goto tma_done;
+                    unsigned char* st = stages + s * kFStageBytes + 16384;
+                    tc::mbar_arrive_tx(&sh->full_tma[s], 16384);
+                    const int y = t0 + c * kFRing;
 #pragma unroll
                     for (int par = 0; par < 2; ++par)
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
-                            tc::tma_load_3d(st + (par * 2 + 0) * 8192 + h * 4096, &xh_map, h * 64, y, 2 * m + par,
+                            tc::tma_load_3d(st + (par * 2 + 0) * 4096 + h * 2048, &xh_map, h * 64, y, 2 * m + par,
                                             &sh->full_tma[s]);
-                            tc::tma_load_3d(st + (par * 2 + 1) * 8192 + h * 4096, &xl_map, h * 64, y, 2 * m + par,
+                            tc::tma_load_3d(st + (par * 2 + 1) * 4096 + h * 2048, &xl_map, h * 64, y, 2 * m + par,
                                             &sh->full_tma[s]);
                         }
                 }
             }
         tma_done:
-            tma_drain(sh, it, err);
+            tma_drain(sh, it, kFStages);
         }
     } else if (warp == 1) {
-        // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_bf16(128, kTcCols, true, true);
             int it = 0, tcount = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
                 const int m = tiles[t].x;
-                const int t0 = first_ring_for_m(m, nside);
-                const int nch = (NP - t0 + kTcRingChunk - 1) / kTcRingChunk;
+                const int nch = nchunks(m);
                 const int a = tcount & 1;
+                TCP_T0(w2);
                 if (!tc::mbar_wait(&sh->acc_empty[a], ((tcount >> 1) & 1) ^ 1, err, 12)) break;
+                TCP_ADD(0, 2, w2);
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + a * 2 * kTcCols;
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kTcStages;
-                    const uint32_t ph = (it / kTcStages) & 1;
+                    const int s = it % kFStages;
+                    const uint32_t ph = (it / kFStages) & 1;
+                    TCP_T0(w0);
                     if (!tc::mbar_wait(&sh->full_tma[s], ph, err, 13)) goto mma_done;
+                    TCP_ADD(0, 0, w0);
+                    TCP_T0(w1);
                     if (!tc::mbar_wait(&sh->full_prod[s], ph, err, 14)) goto mma_done;
+                    TCP_ADD(0, 1, w1);
                     tc::tc_fence_after();
-                    const uint32_t sa = tc::smem_u32(stages + s * kTcStageBytes);
-                    const uint32_t sb = sa + 32768;
+                    const uint32_t sa = tc::smem_u32(stages + s * kFStageBytes);
+                    const uint32_t sb = sa + 16384;
 #pragma unroll
                     for (int par = 0; par < 2; ++par) {
                         const uint32_t d = dbase + par * kTcCols;
-#pragma unroll
-                        for (int ks = 0; ks < 2; ++ks) {
-                            const uint64_t ah = tc::smem_desc_sw128(sa + (par * 2 + 0) * 8192 + ks * 2048, 4096, 1024);
-                            const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * 8192 + ks * 2048, 4096, 1024);
-                            const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 8192 + ks * 2048, 4096, 1024);
-                            const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 8192 + ks * 2048, 4096, 1024);
-                            tc::mma_bf16(d, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-                            tc::mma_bf16(d, ah, bl, idesc, 1u);
-                            tc::mma_bf16(d, al, bh, idesc, 1u);
-                        }
+                        const uint64_t ah = tc::smem_desc_sw128(sa + (par * 2 + 0) * 4096, 2048, 1024);
+                        const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * 4096, 2048, 1024);
+                        const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 4096, 2048, 1024);
+                        const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 4096, 2048, 1024);
+                        tc::mma_bf16(d, ah, bh, idesc, c > 0 ? 1u : 0u);
+                        tc::mma_bf16(d, ah, bl, idesc, 1u);
+                        tc::mma_bf16(d, al, bh, idesc, 1u);
                     }
                     tc::mma_commit(&sh->empty[s]);
                 }
                 tc::mma_commit(&sh->acc_full[a]);
             }
         mma_done:
-            mma_drain(sh, err);
+            mma_drain(sh);
         }
     } else if (warp >= 4 && warp < 8) {
         // ------------------------------------------------ epilogue: TMEM -> alm
@@ -277,7 +338,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (b < nmaps) *(float2*)(alm + 2 * (((int64_t)b * L + l) * M + m)) = make_float2(0.f, 0.f);
                 }
             }
+            TCP_T0(e0);
             if (!tc::mbar_wait_warp(&sh->acc_full[a], (tcount >> 1) & 1, err, 15)) break;
+            if (lane == 0) TCP_ADD(0, 5, e0);
+            TCP_T0(e1);
             tc::tc_fence_after();
             const int row = ew * 32 + lane;
 #pragma unroll 1
@@ -309,61 +373,114 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sh->acc_empty[a]);
+            if (lane == 0) TCP_ADD(0, 6, e1);
         }
-    } else if (warp >= 8) {
+    } else if (warp >= 8 && warp < 8 + kFStages) {
         // ------------------------------------------------ Pbar producers
-        const int pw = warp - 8;    // 0..7
-        const int grp = pw >> 2;    // chunk parity handled by this group
-        const int q = pw & 3;       // 64-degree block within the tile
-        double2* cfw = coef_s + pw * 64;
-        int it = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int m = tiles[t].x, jb = tiles[t].y;
-            const int l0 = m + jb * kTcFwdDeg;
-            const int l0b = l0 + 64 * q;
-            const int t0 = first_ring_for_m(m, nside);
-            const int nch = (NP - t0 + kTcRingChunk - 1) / kTcRingChunk;
-            // coefficients of this warp's 64 degrees (zero beyond L)
-            __syncwarp();
-            for (int i = lane; i < 64; i += 32) cfw[i] = coef[(int64_t)m * Lpad + min(l0b + i, Lpad - 1)];
-            __syncwarp();
-            for (int c = 0; c < nch; ++c, ++it) {
-                if ((it & 1) != grp) continue;
-                const int s = it % kTcStages;
-                if (!tc::mbar_wait_warp(&sh->empty[s], ((it / kTcStages) & 1) ^ 1, err, 16)) goto prod_done;
-                const int p = t0 + c * kTcRingChunk + lane;
-                const uint32_t sa = tc::smem_u32(stages + s * kTcStageBytes);
-                // A tile layout (per parity, hi/lo): atom (i/64) * 4096 + ring group (lane/8) * 1024
-                const uint32_t rowbase = (uint32_t)((q >> 1) * 4096 + (lane >> 3) * 1024);
-                auto emit = [&](int sidx, const double* ev, const double* od) {
+        const int pw = warp - 8;
+        const int r = lane & 15, bp = lane >> 4;
+        AlphaC* cfw = coef_s + pw * kFCoef;
+        int t = blockIdx.x, c = 0, it = 0, cur_tile = -1;
+        int m = 0, jb = 0, t0 = 0, nch = 0;
+        auto load_tile = [&]() {
+            if (t < ntiles) {
+                const int2 tt = tiles[t];
+                m = tt.x;
+                jb = tt.y;
+                t0 = first_ring_for_m(m, nside);
+                nch = nchunks(m);
+            }
+        };
+        auto to_mine = [&]() {
+            while (t < ntiles) {
+                if (c >= nch) {
+                    t += gridDim.x;
+                    c = 0;
+                    load_tile();
+                    continue;
+                }
+                if (it % kFStages == pw) return;
+                ++c;
+                ++it;
+            }
+        };
+        struct In {
+            double2 s0, s1;
+            double x;
+            int p, l0, tile, m, it, lsm;
+        };
+        auto fetch = [&]() {
+            In in;
+            in.p = t0 + c * kFRing + r;
+            in.l0 = m + jb * kTcFwdDeg;
+            in.tile = t;
+            in.m = m;
+            in.it = it;
+            const int b0 = in.l0 + 128 * bp, b1 = b0 + 64;
+            const bool v = in.p < NP;
+            const int64_t sb = ((int64_t)m * nbk + (b0 - m) / kSeedBlock) * NP + in.p;
+            in.s0 = (v && b0 < L) ? seeds[sb] : make_double2(0.0, 0.0);
+            in.s1 = (v && b1 < L) ? seeds[sb + NP] : make_double2(0.0, 0.0);
+            in.x = v ? zr[in.p] : 0.0;
+            in.lsm = lsmax[m];
+            return in;
+        };
+        load_tile();
+        to_mine();
+        if (t < ntiles) {
+            In cur = fetch();
+            while (true) {
+                const int s = cur.it % kFStages;
+                if (cur.tile != cur_tile) {
+                    // coefficient window of this tile's 256 degrees
+                    __syncwarp();
+                    const AlphaC* src = alphac + (int64_t)cur.m * Lpad + cur.l0;
+                    for (int i = lane; i < kFCoef; i += 32) cfw[i] = src[i];
+                    __syncwarp();
+                    cur_tile = cur.tile;
+                }
+                TCP_T0(pw0);
+                if (!tc::mbar_wait_warp(&sh->empty[s], ((cur.it / kFStages) & 1) ^ 1, err, 16)) break;
+                if (lane == 0) TCP_ADD(0, 3, pw0);
+                TCP_T0(pw1);
+                const uint32_t sa = tc::smem_u32(stages + s * kFStageBytes);
+                const uint32_t gbase = (uint32_t)((r >> 3) * 1024);
+                auto emit = [&](int chain, int sidx, const float* ev, const float* od) {
+                    const int q = 2 * bp + chain;  // 64-degree block within the tile
                     uint4 eh, el, oh, ol;
-                    split8(ev, eh, el);
-                    split8(od, oh, ol);
-                    const uint32_t off = rowbase + tc::sw128_offset(lane & 7, ((q & 1) << 2) + sidx);
-                    st_shared_v4(sa + 0 * 8192 + off, eh);
-                    st_shared_v4(sa + 1 * 8192 + off, el);
-                    st_shared_v4(sa + 2 * 8192 + off, oh);
-                    st_shared_v4(sa + 3 * 8192 + off, ol);
+                    split8f(ev, eh, el);
+                    split8f(od, oh, ol);
+                    const uint32_t off = (uint32_t)((q >> 1) * 2048) + gbase + tc::sw128_offset(r & 7, ((q & 1) << 2) + sidx);
+                    st_shared_v4(sa + 0 * 4096 + off, eh);
+                    st_shared_v4(sa + 1 * 4096 + off, el);
+                    st_shared_v4(sa + 2 * 4096 + off, oh);
+                    st_shared_v4(sa + 3 * 4096 + off, ol);
                 };
-                const bool valid = p < NP && l0b < L;
-                const int64_t mi = (int64_t)m * NP + (valid ? p : 0);
-                const int ls = valid ? lstart[mi] : L;
-                const bool fast = __all_sync(0xffffffffu, !valid || ls <= l0b);
-                if (valid) {
-                    const double2 sd = seeds[((int64_t)m * nbk + (l0b - m) / 64) * NP + p];
-                    const double2 ps = fast ? make_double2(0.0, 0.0) : pstart[mi];
-                    gen_block64(l0b, L, ls, ps, sd, pairs[p].z, cfw, fast, emit);
+                const int b0 = cur.l0 + 128 * bp;
+                const bool fast = cur.l0 >= cur.lsm;  // warp-uniform
+                if (fast) {
+                    gen2_fast(cur.s0, cur.s1, cur.x, cur.x, cfw + 128 * bp, cfw + 128 * bp + 64, emit);
                 } else {
-                    const double z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-                    for (int sidx = 0; sidx < 4; ++sidx) emit(sidx, z8, z8);
+                    const bool v = cur.p < NP;
+                    const int64_t mi = (int64_t)cur.m * NP + (v ? cur.p : 0);
+                    const int ls = v ? lstart[mi] : L;
+                    const double2 ps = v ? pstart[mi] : make_double2(0.0, 0.0);
+                    gen1_slow(0, cur.m, b0, L, Lpad, ls, ps, cur.s0, v ? cur.x : 0.0, coef, emit);
+                    gen1_slow(1, cur.m, b0 + 64, L, Lpad, ls, ps, cur.s1, v ? cur.x : 0.0, coef, emit);
                 }
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sh->full_prod[s]);
+                if (lane == 0) TCP_ADD(0, 4, pw1);
+                // next chunk's inputs: issued after this chunk is published, so the
+                // proxy fence and the release-arrive above never wait on them
+                ++c;
+                ++it;
+                to_mine();
+                if (t >= ntiles) break;
+                cur = fetch();
             }
         }
-    prod_done:;
     }
 
     tc::tc_fence_before();
@@ -377,43 +494,29 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ================================================================== synthesis
 // Ah/Al: bf16 [2M][Lh][128] coefficient operand (row i of (m, par) is degree
 // l = m + 2i + par) via tensor maps; writes E/O into spec[m][par][p][c] (FP32).
+// Tile (m, 128 rings); pipeline chunk = one 64-degree seed block.  Stage:
+//   A_par,hl (Pbar^T, K-major SW64, 128 rings x 32 l, 8 KB) at (par*2+hl)*8192
+//   B_par,hl (coefficients, MN-major SW128, 32 l x 128 cols, 8 KB) at 32768 + ...
+// Chunk it goes to producer pair g = it mod 3 (warps 8+2g, 9+2g), which owns
+// stage g (one barrier phase of run-ahead at most); lane runs rings 32w + lane
+// and 64 + 32w + lane of the tile.
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_inv_tc(const __grid_constant__ CUtensorMap ah_map, const __grid_constant__ CUtensorMap al_map,
-                 float* __restrict__ spec, int C, int L, int M, int Lpad, int nside, const RingPair* __restrict__ pairs,
-                 const int* __restrict__ lstart, const double2* __restrict__ pstart, const double2* __restrict__ coef,
-                 const double2* __restrict__ seeds, const int2* __restrict__ tiles, int ntiles, int* __restrict__ err) {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+                 float* __restrict__ spec, int C, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
+                 const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
+                 const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
+                 const int2* __restrict__ tiles, int ntiles, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // align by pointer arithmetic on the shared array (keeps the shared address space known)
+    unsigned char* base = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     unsigned char* stages = base;
-    double2* coef_s = (double2*)(base + kTcStages * kTcStageBytes);
-    TcShared* sh = (TcShared*)(base + kTcStages * kTcStageBytes + 8 * 1024);
-
+    AlphaC* coef_s = (AlphaC*)(base + kIStages * kIStageBytes);
+    TcShared* sh = (TcShared*)(base + kIStages * kIStageBytes + 8 * 64 * 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = 2 * nside;
     const int nbk = seed_blocks(L);
-
-    if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
-            tc::mbar_init(&sh->full_tma[s], 1);
-            tc::mbar_init(&sh->full_prod[s], 4);
-            tc::mbar_init(&sh->empty[s], 1);
-        }
-        for (int a = 0; a < 2; ++a) {
-            tc::mbar_init(&sh->acc_full[a], 1);
-            tc::mbar_init(&sh->acc_empty[a], 4);
-        }
-        tc::mbar_init(&sh->drain, 1);
-        tc::fence_mbar_init();
-    }
-    if (warp == 1) {
-        tc::tmem_alloc(&sh->tmem_base, 512);
-        tc::tmem_relinquish();
-    }
-    tc::tc_fence_before();
-    __syncthreads();
-    tc::tc_fence_after();
+    tc_setup(sh, kIStages, 2, warp);
     const uint32_t tmem = sh->tmem_base;
-
     auto nchunks = [&](int m) { return m < L ? (L - m + kTcDegChunk - 1) / kTcDegChunk : 0; };
 
     if (warp == 0) {
@@ -425,9 +528,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kTcStages;
-                    if (!tc::mbar_wait(&sh->empty[s], ((it / kTcStages) & 1) ^ 1, err, 21)) goto tma_done;
-                    unsigned char* st = stages + s * kTcStageBytes + 32768;
+                    const int s = it % kIStages;
+                    if (!tc::mbar_wait(&sh->empty[s], ((it / kIStages) & 1) ^ 1, err, 21)) goto tma_done;
+                    unsigned char* st = stages + s * kIStageBytes + 32768;
                     tc::mbar_arrive_tx(&sh->full_tma[s], 32768);
 #pragma unroll
                     for (int par = 0; par < 2; ++par)
@@ -441,27 +544,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             }
         tma_done:
-            tma_drain(sh, it, err);
+            tma_drain(sh, it, kIStages);
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // A (Pbar^T) K-major SW64, B (coefficients) MN-major SW128
             const uint32_t idesc = tc::idesc_bf16(128, kTcCols, false, true);
             int it = 0, tcount = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
                 const int a = tcount & 1;
+                TCP_T0(w2);
                 if (!tc::mbar_wait(&sh->acc_empty[a], ((tcount >> 1) & 1) ^ 1, err, 22)) break;
+                TCP_ADD(1, 2, w2);
                 tc::tc_fence_after();
                 const uint32_t dbase = tmem + a * 2 * kTcCols;
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kTcStages;
-                    const uint32_t ph = (it / kTcStages) & 1;
+                    const int s = it % kIStages;
+                    const uint32_t ph = (it / kIStages) & 1;
+                    TCP_T0(w0);
                     if (!tc::mbar_wait(&sh->full_tma[s], ph, err, 23)) goto mma_done;
+                    TCP_ADD(1, 0, w0);
+                    TCP_T0(w1);
                     if (!tc::mbar_wait(&sh->full_prod[s], ph, err, 24)) goto mma_done;
+                    TCP_ADD(1, 1, w1);
                     tc::tc_fence_after();
-                    const uint32_t sa = tc::smem_u32(stages + s * kTcStageBytes);
+                    const uint32_t sa = tc::smem_u32(stages + s * kIStageBytes);
                     const uint32_t sb = sa + 32768;
 #pragma unroll
                     for (int par = 0; par < 2; ++par) {
@@ -482,7 +590,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc::mma_commit(&sh->acc_full[a]);
             }
         mma_done:
-            mma_drain(sh, err);
+            mma_drain(sh);
         }
     } else if (warp >= 4 && warp < 8) {
         // ------------------------------------------------ epilogue: TMEM -> spec (E, O)
@@ -492,8 +600,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const int m = tiles[t].x, rb = tiles[t].y;
             const int t0 = first_ring_for_m(m, nside);
             const int a = tcount & 1;
-            const int r = rb + ew * 32 + lane;
-            const int p = t0 + r;
+            const int rr = rb + ew * 32 + lane;
+            const int p = t0 + rr;
             if (!tc::mbar_wait_warp(&sh->acc_full[a], (tcount >> 1) & 1, err, 25)) break;
             tc::tc_fence_after();
 #pragma unroll 1
@@ -514,60 +622,111 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sh->acc_empty[a]);
         }
-    } else if (warp >= 8) {
+    } else if (warp >= 8 && warp < 8 + 2 * kIStages) {
         // ------------------------------------------------ Pbar^T producers
         const int pw = warp - 8;
-        const int grp = pw >> 2;  // chunk parity handled by this group
-        const int rw = pw & 3;    // 32-ring slice of the 128-ring tile
-        double2* cfw = coef_s + pw * 64;
-        int it = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int m = tiles[t].x, rb = tiles[t].y;
-            const int t0 = first_ring_for_m(m, nside);
-            const int nch = nchunks(m);
-            const int r = rw * 32 + lane;  // row of the A tile
-            const int p = t0 + rb + r;
-            const bool valid = p < NP;
-            const int64_t mi = (int64_t)m * NP + (valid ? p : 0);
-            const int ls = valid ? lstart[mi] : L;
-            const double x = valid ? pairs[p].z : 0.0;
-            for (int c = 0; c < nch; ++c, ++it) {
-                if ((it & 1) != grp) continue;
-                const int s = it % kTcStages;
-                const int l0b = m + c * kTcDegChunk;
+        const int g = pw >> 1, w = pw & 1;
+        AlphaC* cfw = coef_s + pw * 64;
+        const int r0 = 32 * w + lane, r1 = 64 + 32 * w + lane;  // tile rows of the two chains
+        int t = blockIdx.x, c = 0, it = 0;
+        int m = 0, rb = 0, t0 = 0, nch = 0;
+        auto load_tile = [&]() {
+            if (t < ntiles) {
+                const int2 tt = tiles[t];
+                m = tt.x;
+                rb = tt.y;
+                t0 = first_ring_for_m(m, nside);
+                nch = nchunks(m);
+            }
+        };
+        auto to_mine = [&]() {
+            while (t < ntiles) {
+                if (c >= nch) {
+                    t += gridDim.x;
+                    c = 0;
+                    load_tile();
+                    continue;
+                }
+                if (it % kIStages == g) return;
+                ++c;
+                ++it;
+            }
+        };
+        struct In {
+            double2 s0, s1;
+            double x0, x1;
+            AlphaC c0, c1;
+            int p0, p1, l0b, m, it, lsm;
+        };
+        auto fetch = [&]() {
+            In in;
+            in.m = m;
+            in.it = it;
+            in.l0b = m + c * kTcDegChunk;
+            in.p0 = t0 + rb + r0;
+            in.p1 = t0 + rb + r1;
+            const int64_t sb = ((int64_t)m * nbk + c) * NP;
+            in.s0 = in.p0 < NP ? seeds[sb + in.p0] : make_double2(0.0, 0.0);
+            in.s1 = in.p1 < NP ? seeds[sb + in.p1] : make_double2(0.0, 0.0);
+            in.x0 = in.p0 < NP ? zr[in.p0] : 0.0;
+            in.x1 = in.p1 < NP ? zr[in.p1] : 0.0;
+            const AlphaC* src = alphac + (int64_t)m * Lpad + in.l0b;
+            in.c0 = src[lane];
+            in.c1 = src[lane + 32];
+            in.lsm = lsmax[m];
+            return in;
+        };
+        load_tile();
+        to_mine();
+        if (t < ntiles) {
+            In cur = fetch();
+            while (true) {
+                const int s = cur.it % kIStages;
+                TCP_T0(pw0);
+                if (!tc::mbar_wait_warp(&sh->empty[s], ((cur.it / kIStages) & 1) ^ 1, err, 26)) break;
+                if (lane == 0) TCP_ADD(1, 3, pw0);
+                TCP_T0(pw1);
                 __syncwarp();
-                for (int i = lane; i < 64; i += 32) cfw[i] = coef[(int64_t)m * Lpad + min(l0b + i, Lpad - 1)];
+                cfw[lane] = cur.c0;
+                cfw[lane + 32] = cur.c1;
                 __syncwarp();
-                if (!tc::mbar_wait_warp(&sh->empty[s], ((it / kTcStages) & 1) ^ 1, err, 26)) goto prod_done;
-                const uint32_t sa = tc::smem_u32(stages + s * kTcStageBytes);
-                // K-major SW64: row r (ring), 32 bf16 per row; 8-row groups of 512 B
-                const uint32_t rowbase = (uint32_t)((r >> 3) * 512);
-                auto emit = [&](int sidx, const double* ev, const double* od) {
+                const uint32_t sa = tc::smem_u32(stages + s * kIStageBytes);
+                auto emit = [&](int chain, int sidx, const float* ev, const float* od) {
+                    const int rr = chain ? r1 : r0;
                     uint4 eh, el, oh, ol;
-                    split8(ev, eh, el);
-                    split8(od, oh, ol);
-                    const uint32_t off = rowbase + tc::sw64_offset(r & 7, sidx);
+                    split8f(ev, eh, el);
+                    split8f(od, oh, ol);
+                    const uint32_t off = (uint32_t)((rr >> 3) * 512) + tc::sw64_offset(rr & 7, sidx);
                     st_shared_v4(sa + 0 * 8192 + off, eh);
                     st_shared_v4(sa + 1 * 8192 + off, el);
                     st_shared_v4(sa + 2 * 8192 + off, oh);
                     st_shared_v4(sa + 3 * 8192 + off, ol);
                 };
-                const bool fast = __all_sync(0xffffffffu, !valid || ls <= l0b);
-                if (valid) {
-                    const double2 sd = seeds[((int64_t)m * nbk + c) * NP + p];
-                    const double2 ps = fast ? make_double2(0.0, 0.0) : pstart[mi];
-                    gen_block64(l0b, L, ls, ps, sd, x, cfw, fast, emit);
+                if (cur.l0b >= cur.lsm) {
+                    TCP_T0(gg);
+                    gen2_fast(cur.s0, cur.s1, cur.x0, cur.x1, cfw, cfw, emit);
+                    if (lane == 0) TCP_ADD(1, 5, gg);
                 } else {
-                    const double z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-                    for (int sidx = 0; sidx < 4; ++sidx) emit(sidx, z8, z8);
+                    const bool v0 = cur.p0 < NP, v1 = cur.p1 < NP;
+                    const int64_t mb = (int64_t)cur.m * NP;
+                    gen1_slow(0, cur.m, cur.l0b, L, Lpad, v0 ? lstart[mb + cur.p0] : L,
+                              v0 ? pstart[mb + cur.p0] : make_double2(0.0, 0.0), cur.s0, cur.x0, coef, emit);
+                    gen1_slow(1, cur.m, cur.l0b, L, Lpad, v1 ? lstart[mb + cur.p1] : L,
+                              v1 ? pstart[mb + cur.p1] : make_double2(0.0, 0.0), cur.s1, cur.x1, coef, emit);
                 }
+                TCP_T0(ff);
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sh->full_prod[s]);
+                if (lane == 0) TCP_ADD(1, 6, ff);
+                if (lane == 0) TCP_ADD(1, 4, pw1);
+                ++c;
+                ++it;
+                to_mine();
+                if (t >= ntiles) break;
+                cur = fetch();
             }
         }
-    prod_done:;
     }
 
     tc::tc_fence_before();

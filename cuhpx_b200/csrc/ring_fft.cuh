@@ -285,14 +285,19 @@ __device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, c
     group_sync(tpf, g);
 }
 
-// Inverse transform of spectrum Fs[0..mt) (shared memory) into one real ring x[0..n).
+// Inverse transform of the ring spectrum Fg[0..mt) (global) into one real ring
+// x[0..n).  The spectrum is staged once, contiguously, into buf2 (free until
+// the DFT starts), because each output needs both F[k] and F[h-k].
 // ref != nullptr: write ref - x (Jacobi residual).
 template <typename T>
-__device__ void ring_inverse(const cplx<T>* Fs, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ x,
+__device__ void ring_inverse(const cplx<T>* __restrict__ Fg, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ x,
                              const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ twP,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
                              const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h, mt = rp.mt;
+    for (int k = lt; k < mt; k += tpf) buf2[k] = Fg[k];
+    group_sync(tpf, g);
+    const cplx<T>* Fs = buf2;
     for (int k = lt; k < h; k += tpf) {
         // X_k and conj(X_{h-k}) with the phase e^{+i s k pi/n}; imag of X_0, X_h dropped
         cplx<T> Xa = {(T)0, (T)0}, Xb = {(T)0, (T)0};

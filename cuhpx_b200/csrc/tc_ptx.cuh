@@ -2,9 +2,11 @@
 // TMEM allocation, UMMA shared-memory / instruction descriptors, MMA issue and
 // commit, TMEM loads, mbarriers with bounded waits, and TMA tile loads.
 //
-// Every wait here is bounded: after kSpinLimit polls it records an error code
-// in the caller's flag and gives up, so a broken pipeline ends the kernel with
-// a status the host can read instead of hanging the GPU.
+// Every wait here is bounded: after kWaitLimitNs of %globaltimer time it records
+// an error code in the caller's flag and gives up, so a broken pipeline ends
+// the kernel with a status the host can read instead of hanging the GPU.  Polls
+// suspend in hardware (suspend-time hint), and the flag and the clock are only
+// read every 16 polls, so waiting warps cost almost nothing.
 #pragma once
 
 #include <cuda.h>
@@ -15,7 +17,13 @@
 namespace hpx {
 namespace tc {
 
-constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;\n" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -32,23 +40,44 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
                  "r"(bytes)
                  : "memory");
 }
+// try_wait with a suspend-time hint: a waiting thread is parked by the hardware
+// (for at most kSuspendHintNs) until the phase completes, instead of spinning
+// and taking issue slots from the producer warps on the same SM sub-partition.
+constexpr uint32_t kSuspendHintNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
 // Bounded wait; on timeout sets *err (if not set) and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 1;; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (*(volatile int*)err) return false;
+        if ((i & 15) == 0) {
+            if (*(volatile int*)err) return false;
+            if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                atomicCAS(err, 0, code);
+                return false;
+            }
+        }
     }
-    atomicCAS(err, 0, code);
-    return false;
+}
+
+// Bounded wait without an error flag (exit drains): true if the phase completed.
+__device__ __forceinline__ bool mbar_wait_quiet(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 15) == 0 && globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    }
 }
 
 // Warp-uniform bounded wait: lane 0 polls, every lane gets the same answer, so
