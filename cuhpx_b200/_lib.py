@@ -60,6 +60,7 @@ SIGNATURES = {
     "hpx_sht_forward_adjoint": ([_vp, _vp, _vp, _i64, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_inverse_adjoint": ([_vp, _vp, _vp, _i64, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_refined": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
+    "hpx_sht_forward_noalloc": ([_vp, _vp, _vp, _i64, _vp], ctypes.c_int),
     "hpx_plan_info": (
         [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
         ctypes.c_int,

@@ -497,6 +497,9 @@ struct Pipeline {
         c += (P->tcA_bytes() + 255) & ~(size_t)255;
         F = (T*)c;
     }
+    // analysis-only layout: folded spectra and ring spectra at given addresses
+    Pipeline(const hpx_plan_s* p, T* spec_, T* F_, cudaStream_t s)
+        : P(p), st(s), spec(spec_), almT(nullptr), resid(nullptr), tcA(nullptr), F(F_) {}
     T* F;  // ring-major spectra [map][Ftot] complex
     // folded spectra as bf16 hi/lo (mixed plans), aliasing the spec region
     uint32_t* xh() const { return P->mixed() ? (uint32_t*)spec : nullptr; }
@@ -678,9 +681,93 @@ int dispatch(hpx_plan_t plan, Op op, const void* in, void* out, int64_t batch, v
     }
 }
 
+// ---- analysis without allocation: one static scratch array per device
+//
+// Region sizes of one chunk of batch_chunk maps: folded spectra, then ring
+// spectra, each 256-byte aligned.  Every scratch element a call reads was
+// written earlier in the same call (ring spectra for the rings that carry an
+// order, folded spectra for every column of the chunk), so nothing has to
+// start at zero.
+size_t noalloc_spec_offset(const hpx_plan_s* P) { return (P->spec_bytes() + 255) & ~(size_t)255; }
+size_t noalloc_need(const hpx_plan_s* P) { return noalloc_spec_offset(P) + P->F_bytes(); }
+
+}  // namespace
+
+// Zero-initialised device storage of the module: no allocation call makes it,
+// it exists once per device the library is loaded on, and every plan on that
+// device shares it.
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Address of the scratch on `device`, looked up once per device with that
+// device current (the caller holds a DeviceGuard for it).
+int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return set_err(HPX_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return set_err(HPX_ERR_CUDA, std::string("scratch symbol address: ") + cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[device] = p;
+    }
+    *out = (unsigned char*)g_noalloc_ptr[device];
+    return HPX_OK;
+}
+
+template <typename T>
+int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch, unsigned char* scratch,
+                        cudaStream_t st) {
+    Pipeline<T> pl(P, (T*)scratch, (T*)(scratch + noalloc_spec_offset(P)), st);
+    const int64_t bc = P->batch_chunk;
+    const size_t alm_stride = (size_t)P->L * P->M * 2;
+    for (int64_t b0 = 0; b0 < batch; b0 += bc) {
+        const int nb = (int)std::min<int64_t>(bc, batch - b0);
+        pl.ring_fwd((const T*)in + b0 * P->npix, nb, 0);
+        pl.leg_fwd((T*)out + b0 * alm_stride, nb, 0);
+        if (pl.rc != HPX_OK) return pl.rc;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(HPX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    return HPX_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream) {
+    if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
+    if (batch < 0) return set_err(HPX_ERR_INVALID_ARG, "negative batch");
+    if (batch == 0) return HPX_OK;
+    if (!map || !alm) return set_err(HPX_ERR_INVALID_ARG, "null data pointer");
+    const size_t need = noalloc_need(plan);
+    if (need > kNoAllocScratchBytes)
+        return set_err(HPX_ERR_WORKSPACE, "hpx_sht_forward_noalloc: this plan needs " + std::to_string(need) +
+                                              " bytes of scratch per chunk of " + std::to_string(plan->batch_chunk) +
+                                              " maps, above the static scratch of " +
+                                              std::to_string(kNoAllocScratchBytes) +
+                                              " bytes; use hpx_sht_forward with a workspace");
+    DeviceGuard g(plan->device);
+    unsigned char* scratch = nullptr;
+    int rc = noalloc_scratch(plan->device, &scratch);
+    if (rc != HPX_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        return plan->f64 ? run_forward_noalloc<double>(plan, map, alm, batch, scratch, st)
+                         : run_forward_noalloc<float>(plan, map, alm, batch, scratch, st);
+    } catch (const std::exception& ex) {
+        return set_err(HPX_ERR_CUDA, ex.what());
+    }
+}
 
 int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan) {
     if (!desc || !plan) return set_err(HPX_ERR_INVALID_ARG, "null argument");

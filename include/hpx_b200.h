@@ -107,6 +107,23 @@ HPX_API int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void*
 HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch,
                             void* workspace, size_t workspace_bytes, void* stream);
 
+/* Forward SHT (analysis) that allocates nothing and takes no workspace.  No
+ * counterpart in cuHPX: it is added for callers that cannot hand the library
+ * device memory, such as an FFI host with no device allocator of its own, or a
+ * loop whose allocator may not be called because cudaMalloc/cudaFree
+ * synchronise the device and would stall the other streams' work.
+ * It runs the same kernels as hpx_sht_forward, with the ring and folded spectra
+ * of one chunk of batch_chunk maps kept in one static device array of
+ * 32 MiB (33554432 bytes) per device, shared by every plan and call on that
+ * device.  A plan whose chunk needs more (per chunk of 64 maps: about 28 MiB at
+ * nside 64, lmax = mmax = 128 for FP32/BF16X3; FP64 twice that) is refused with
+ * HPX_ERR_WORKSPACE before anything runs.  Nothing in the array has to start
+ * at zero.  Calls that overlap in time -- on two streams, or from two threads --
+ * race on the array and give wrong results: serialise them.  The first call on
+ * a device looks up the array's address (cudaGetSymbolAddress, with the plan's
+ * device current); make that first call before any stream capture. */
+HPX_API int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream);
+
 /* Per-kernel timing.  While enabled, every kernel the plan launches is
  * bracketed by CUDA events recorded on the launch stream; hpx_stats_read
  * synchronises on those events and returns, per stage, the number of launches
