@@ -6,7 +6,7 @@ Inputs are band-limited Gaussian fields (C_l ~ (l+1)^-2) plus N(0, 1e-3)
 white noise, generated on the device from a fixed seed; each batch is 3.2 GB,
 larger than the 126 MB L2, so no flush is needed between steps.
 
-  python bench.py [--gpus N --steps K --warmup W] [--precision bf16x3|tf32|fp32] [--refine k]
+  python bench.py [--gpus N --steps K --warmup W] [--precision f16x3|bf16x3|fp32] [--refine k]
   python bench.py --impl reference ...   # the reference's CPU algorithm (oracle port) on the host
 
 Under torchrun every rank runs its own batch (replicas, no collective on the
@@ -35,7 +35,7 @@ METRIC = "SHT+iSHT maps/s nside1024 lmax2047 B64: mixed vs FP32 plain, err<=1e-5
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hpx", choices=["hpx", "reference"])
     ap.add_argument("--precision", default="auto")
@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the error check against the FP64 path")
+    ap.add_argument("--accuracy-maps", type=int, default=2)
     ap.add_argument("--cpu-sample-m", type=int, default=12)
     return ap.parse_args()
 
@@ -66,7 +68,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL,
                 text=True,
@@ -244,7 +246,7 @@ def run_gpu(args):
     nside, L, B = args.nside, args.lmax, args.batch
     prec = args.precision
     if prec == "auto":
-        prec = "bf16x3" if _tc_available(hpx, dev) else "fp32"
+        prec = "f16x3" if _tc_available(hpx, dev) else "fp32"
     refine = args.refine if args.refine >= 0 else (1 if prec in ("bf16x3", "tf32") else 0)
 
     f = make_inputs(torch, hpx, nside, L, B, dev)
@@ -316,6 +318,10 @@ def run_gpu(args):
         nb = f.numel() * f.element_size()
         e2e = {"value": world * B * max(1, args.steps // 2) / (ms_e / 1000.0), "unit": "maps/s", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb}
 
+    acc = None
+    if not args.no_accuracy:
+        acc = accuracy_vs_fp64(torch, hpx, sht, isht, f[: args.accuracy_maps], nside, L, refine)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(nside, L, args.cpu_sample_m)
@@ -354,6 +360,7 @@ def run_gpu(args):
             "cpu_baseline": cpu,
             "plain_fp32_maps_per_s": plain,
             "check_rel_l2_vs_fp32": check_rel,
+            "err_vs_fp64": acc,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -362,9 +369,36 @@ def run_gpu(args):
     return 0
 
 
+def accuracy_vs_fp64(torch, hpx, sht, isht, f, nside, L, refine):
+    """Rel-L2 of the timed modules against the FP64 path with the same Jacobi
+    iterations, on a few of the timed maps: the analysis coefficients and the
+    round trip iSHT(SHT(f))."""
+
+    def rel(a, b):
+        return float((a.to(b.dtype) - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt())
+
+    with torch.no_grad():
+        f64 = f.double()
+        a64 = hpx.SHTCUDA(nside, lmax=L, mmax=L, refine_iters=refine)(f64)
+        r64 = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(a64)
+        a = sht(f)
+        r = isht(a)
+        out = {
+            "maps": int(f.shape[0]),
+            "refine_iters": refine,
+            "alm_rel_l2": rel(a, a64),
+            "roundtrip_rel_l2": rel(r, r64),
+            "tolerance": 1e-5,
+            "reference": "this library's FP64 path (FP64 FFTs, FP64 Legendre recurrence and contraction), same refine_iters",
+        }
+        del f64, a64, r64
+    torch.cuda.empty_cache()
+    return out
+
+
 def _tc_available(hpx, dev):
     try:
-        hpx.get_plan(8, 17, 17, "ring", "bf16x3", dev.index)
+        hpx.get_plan(8, 17, 17, "ring", "f16x3", dev.index)
         return True
     except Exception:
         return False
@@ -400,9 +434,10 @@ def roofline(stats, args, prec, refine, nside, L, B):
     chunk = min(B, 64)
     if name.startswith("legendre"):
         useful = flops_map * chunk
-        if prec in ("bf16x3", "tf32"):
-            terms = 3 if prec == "bf16x3" else 1
-            peak = peaks.get("bf16_tflops", 1590.0) if prec == "bf16x3" else peaks.get("bf16_tflops", 1590.0) / 2
+        if prec in ("bf16x3", "f16x3", "tf32"):
+            terms = 1 if prec == "tf32" else 3
+            # fp16 and bf16 run at the same tcgen05 kind::f16 rate
+            peak = peaks.get("bf16_tflops", 1590.0) if prec != "tf32" else peaks.get("bf16_tflops", 1590.0) / 2
             achieved = useful * terms / (per_launch_ms * 1e-3) / 1e12
             return {
                 "kernel": name,

@@ -22,7 +22,7 @@ STATUS = {
     6: "workspace too small",
 }
 
-PRECISIONS = {"fp32": 0, "fp64": 1, "bf16x3": 2, "tf32": 3}
+PRECISIONS = {"fp32": 0, "fp64": 1, "bf16x3": 2, "tf32": 3, "f16x3": 4}
 
 # exported symbols and their signatures (argtypes, restype)
 _vp = ctypes.c_void_p

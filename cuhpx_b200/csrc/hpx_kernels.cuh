@@ -20,7 +20,8 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
                                                   T* __restrict__ F, int64_t Ftot, int nside,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
                                                   int logPmax, const cplx<T>* __restrict__ gtab,
-                                                  const cplx<T>* __restrict__ chirp) {
+                                                  const cplx<T>* __restrict__ chirp,
+                                                  unsigned* __restrict__ fmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = 2 * nside, R = 4 * nside - 1;
     const int t = blockIdx.x;
@@ -45,9 +46,17 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
     const int64_t np = npix(nside);
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
-    for (int b = b0 + g; b < b1; b += S)
-        ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff), rp, twP,
-                     gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+    for (int b = b0 + g; b < b1; b += S) {
+        const T mx = ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff),
+                                  rp, twP, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+        if (fmax) {
+            // per-map max |F| (scale of the FP16 operands); a group is whole warps
+            float v = (float)mx;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if ((threadIdx.x & 31) == 0 && v > 0.f) atomicMax(fmax + b, __float_as_uint(v));
+        }
+    }
 }
 
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
@@ -88,10 +97,37 @@ __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64
                      chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
 }
 
+// Per-map max |x| over rows of n floats: atomicMax of the float bits into out[map]
+// (out zeroed by the caller).  Grid (blocks per row, maps).
+__global__ void __launch_bounds__(256) k_rows_maxabs(const float* __restrict__ x, int64_t n,
+                                                     unsigned* __restrict__ out) {
+    const int b = blockIdx.y;
+    const float* row = x + (int64_t)b * n;
+    float v = 0.f;
+    const int64_t n4 = ((((uintptr_t)row) & 15) == 0) ? n / 4 : 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 q = *(const float4*)(row + 4 * i);
+        v = fmaxf(v, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)), fmaxf(fabsf(q.z), fabsf(q.w))));
+    }
+    for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v = fmaxf(v, fabsf(row[i]));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ float red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = fmaxf(v, red[w]);
+        if (v > 0.f) atomicMax(out + b, __float_as_uint(v));
+    }
+}
+
 // Fold ring spectra into the m-major Legendre operand:
 //   S = c (F_t + F_t'),  D = c (F_t - F_t')   (equator: S = c F_t, D = 0)
 // with c = w_t (analysis) or c_m = 2, 1 at m = 0 and m = nphi/2 (adjoint of synthesis).
-// Output spec[m][par][p][col] in T, or bf16 hi/lo pairs xh/xl (mixed plans).
+// Output spec[m][par][p][col] in T, or hi/lo pairs xh/xl (mixed plans): bf16,
+// or, with fmax given, fp16 of the values times 2^e(map), e from the map's
+// max |F| (recorded by k_ring_fwd) times the bound wb on |c| (F_t + F_t').
 // CTA per (block of 32 orders, ring pair); the transpose goes through shared memory.
 template <typename T>
 constexpr int fold_mb() { return sizeof(T) == 4 ? 32 : 16; }
@@ -99,7 +135,8 @@ constexpr int fold_mb() { return sizeof(T) == 4 ? 32 : 16; }
 template <typename T>
 __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t Ftot, int nmaps, int nside,
                                               const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ spec,
-                                              int C, uint32_t* __restrict__ xh, uint32_t* __restrict__ xl) {
+                                              int C, uint32_t* __restrict__ xh, uint32_t* __restrict__ xl,
+                                              const unsigned* __restrict__ fmax, float wb) {
     constexpr int MB = fold_mb<T>();
     __shared__ cplx<T> tn[64][MB + 1];
     __shared__ cplx<T> ts[64][MB + 1];
@@ -135,7 +172,19 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
         }
         const int64_t i0 = (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b;
         const int64_t i1 = (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b;
-        if (xh) {
+        if (xh && fmax) {
+            // FP16 operands scaled by 2^e(map); |S|, |D| <= wb * max|F|
+            const float sc = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? fmax[b] : 0u) * wb));
+            uint16_t h0, l0, h1, l1;
+            tc::split_f16((float)S.re * sc, h0, l0);
+            tc::split_f16((float)S.im * sc, h1, l1);
+            xh[i0 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+            xl[i0 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+            tc::split_f16((float)D.re * sc, h0, l0);
+            tc::split_f16((float)D.im * sc, h1, l1);
+            xh[i1 >> 1] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+            xl[i1 >> 1] = (uint32_t)l0 | ((uint32_t)l1 << 16);
+        } else if (xh) {
             uint16_t h0, l0, h1, l1;
             tc::split_bf16((float)S.re, h0, l0);
             tc::split_bf16((float)S.im, h1, l1);

@@ -103,6 +103,7 @@ struct hpx_plan_s {
     AlphaC* d_alphac = nullptr;  // [M][Lpad] block-normalised recurrence (tensor-core producers)
     int* d_lsmax = nullptr;      // per order: max over its rings of the first significant degree
     int n_fwdtiles = 0;
+    float wmax = 0.f;            // largest ring weight w_t
     size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
@@ -163,9 +164,12 @@ struct hpx_plan_s {
     size_t almT_bytes() const { return (size_t)M * L * cols() * real_size(); }
     size_t resid_bytes() const { return (size_t)batch_chunk * npix * real_size(); }
     size_t F_bytes() const { return (size_t)batch_chunk * Ftot * 2 * real_size(); }
-    bool mixed() const { return prec == HPX_PREC_BF16X3; }
-    // bf16 hi/lo synthesis operand [2M][Lh][128] x 2
+    bool mixed() const { return prec == HPX_PREC_BF16X3 || prec == HPX_PREC_F16X3; }
+    bool f16() const { return prec == HPX_PREC_F16X3; }
+    // bf16/fp16 hi/lo synthesis operand [2M][Lh][128] x 2
     size_t tcA_bytes() const { return mixed() ? (size_t)2 * 2 * M * tc.Lh * kTcCols * sizeof(uint16_t) : 0; }
+    // per-map max |F| and max |a| (FP16 operand scales)
+    size_t scale_bytes() const { return f16() ? (size_t)2 * 4 * batch_chunk : 0; }
 };
 
 namespace {
@@ -265,13 +269,16 @@ int tc_create(hpx_plan_s* P) {
         HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * it.size()));
         HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
     }
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
     T.active = 1;
     return HPX_OK;
 }
 
-// 3-D bf16 tensor map over [outer][rows][128 cols] with a {64 cols, box_rows} box, 128B swizzle.
+// 3-D tensor map of 2-byte elements (bf16 or fp16 halves; TMA only moves bytes) over
+// [outer][rows][128 cols] with a {64 cols, box_rows} box, 128B swizzle.
 int encode_operand(const hpx_plan_s* P, CUtensorMap* map, void* base, uint64_t rows, uint64_t outer, int box_rows) {
     const cuuint64_t dims[3] = {(cuuint64_t)kTcCols, rows, outer};
     const cuuint64_t strides[2] = {(cuuint64_t)kTcCols * 2, (cuuint64_t)kTcCols * 2 * rows};
@@ -345,6 +352,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
         // threads per FFT: ~16 points per thread, between one warp and the CTA
         rp.tpf = std::min(256, std::max(32, Pf / 16));
         mtmax = std::max(mtmax, rp.mt);
+        P->wmax = std::max(P->wmax, (float)rp.w);
     }
     // ring-major spectrum offsets: north rings 0..NP-1, then south rings
     int64_t foff = 0;
@@ -453,7 +461,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
 
     int rc = P->f64 ? create_typed<double>(P) : create_typed<float>(P);
     if (rc != HPX_OK) return rc;
-    if (P->prec == HPX_PREC_TF32) return set_err(HPX_ERR_UNSUPPORTED, "tf32 contraction is not built; use bf16x3");
+    if (P->prec == HPX_PREC_TF32) return set_err(HPX_ERR_UNSUPPORTED, "tf32 contraction is not built; use f16x3 or bf16x3");
     if (P->mixed()) {
         rc = tc_create(P);
         if (rc != HPX_OK) return rc;
@@ -482,7 +490,10 @@ struct Pipeline {
     T* spec;
     T* almT;
     T* resid;
-    uint16_t* tcA;  // bf16 hi/lo synthesis operand (mixed plans)
+    uint16_t* tcA;  // bf16/fp16 hi/lo synthesis operand (mixed plans)
+    unsigned* fmax = nullptr;  // per-map max |F| (FP16 plans)
+    unsigned* amax = nullptr;  // per-map max |a| (FP16 plans)
+    float fold_wb = 0.f;       // bound on the fold factor |c| (F_t + F_t') / max|F|
     int rc = HPX_OK;
 
     Pipeline(const hpx_plan_s* p, void* ws, cudaStream_t s) : P(p), st(s) {
@@ -496,10 +507,19 @@ struct Pipeline {
         tcA = (uint16_t*)c;
         c += (P->tcA_bytes() + 255) & ~(size_t)255;
         F = (T*)c;
+        c += (P->F_bytes() + 255) & ~(size_t)255;
+        set_scales(c);
+    }
+    void set_scales(char* c) {
+        if (!P->f16()) return;
+        fmax = (unsigned*)c;
+        amax = fmax + P->batch_chunk;
     }
     // analysis-only layout: folded spectra and ring spectra at given addresses
-    Pipeline(const hpx_plan_s* p, T* spec_, T* F_, cudaStream_t s)
-        : P(p), st(s), spec(spec_), almT(nullptr), resid(nullptr), tcA(nullptr), F(F_) {}
+    Pipeline(const hpx_plan_s* p, T* spec_, T* F_, char* scales, cudaStream_t s)
+        : P(p), st(s), spec(spec_), almT(nullptr), resid(nullptr), tcA(nullptr), F(F_) {
+        set_scales(scales);
+    }
     T* F;  // ring-major spectra [map][Ftot] complex
     // folded spectra as bf16 hi/lo (mixed plans), aliasing the spec region
     uint32_t* xh() const { return P->mixed() ? (uint32_t*)spec : nullptr; }
@@ -536,14 +556,18 @@ struct Pipeline {
         const int g = maps_per_cta_ring();
         {
             Timer tm(P, st, kStRingFwd);
+            if (fmax) cudaMemsetAsync(fmax, 0, sizeof(unsigned) * nb, st);
             dim3 grid(P->R, (nb + g - 1) / g);
             k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->nside, P->d_pairs,
                                                           (const cplx<T>*)P->d_tw, P->logPmax,
-                                                          (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp);
+                                                          (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, fmax);
         }
         Timer tm(P, st, kStFold);
+        // |c (F_t +- F_t')| <= 2 max|c| max|F|: c = w_t, or c_m <= 2 for the adjoint
+        fold_wb = adjoint ? 4.f : 2.f * P->wmax;
         dim3 fg((P->mtmax + fold_mb<T>() - 1) / fold_mb<T>(), P->NP, (nb + 63) / 64);
-        k_fold<T><<<fg, 256, 0, st>>>(F, P->Ftot, nb, P->nside, P->d_pairs, adjoint, spec, P->cols(), xh(), xl());
+        k_fold<T><<<fg, 256, 0, st>>>(F, P->Ftot, nb, P->nside, P->d_pairs, adjoint, spec, P->cols(), xh(), xl(),
+                                      fmax, fold_wb);
     }
     // synthesis output spec (E/O) -> ring spectra F -> map (ref: residual ref - map)
     void ring_inv(T* map, int nb, int adjoint, const T* ref) {
@@ -570,9 +594,11 @@ struct Pipeline {
             CUtensorMap mh, ml;
             if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
-            k_leg_fwd_tc<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kFSmem, st>>>(
+            auto kern = P->f16() ? k_leg_fwd_tc<true> : k_leg_fwd_tc<false>;
+            kern<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kFSmem, st>>>(
                 mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
-                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, TP.d_err);
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, fmax,
+                fold_wb, TP.d_err);
             return;
         }
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
@@ -588,8 +614,14 @@ struct Pipeline {
             uint16_t* al = tcA + (size_t)2 * P->M * TP.Lh * kTcCols;
             {
                 Timer tm(P, st, kStAlmCols);
+                if (amax) {
+                    cudaMemsetAsync(amax, 0, sizeof(unsigned) * nb, st);
+                    const int64_t n = (int64_t)P->L * P->M * 2;
+                    const int bx = (int)std::min<int64_t>(64, (n / 4 + 1023) / 1024);
+                    k_rows_maxabs<<<dim3(std::max(bx, 1), nb), 256, 0, st>>>((const float*)alm, n, amax);
+                }
                 dim3 tg((P->M + 31) / 32, P->L + 64);
-                k_alm_to_tc<<<tg, dim3(32, 8), 0, st>>>((const float*)alm, nb, P->L, P->M, TP.Lh, ah, al);
+                k_alm_to_tc<<<tg, dim3(32, 8), 0, st>>>((const float*)alm, nb, P->L, P->M, TP.Lh, ah, al, amax);
             }
             Timer tm(P, st, kStLegInv);
             // orders the tensor cores do not visit must read as zero in the ring stage
@@ -600,9 +632,10 @@ struct Pipeline {
             CUtensorMap mh, ml;
             if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
-            k_leg_inv_tc<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kISmem, st>>>(
-                mh, ml, (float*)spec, C, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
-                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, TP.d_err);
+            auto kern = P->f16() ? k_leg_inv_tc<true> : k_leg_inv_tc<false>;
+            kern<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kISmem, st>>>(
+                mh, ml, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, amax, TP.d_err);
             return;
         }
         dim3 tg((P->M + 31) / 32, P->L, (nb + 15) / 16);
@@ -689,7 +722,10 @@ int dispatch(hpx_plan_t plan, Op op, const void* in, void* out, int64_t batch, v
 // order, folded spectra for every column of the chunk), so nothing has to
 // start at zero.
 size_t noalloc_spec_offset(const hpx_plan_s* P) { return (P->spec_bytes() + 255) & ~(size_t)255; }
-size_t noalloc_need(const hpx_plan_s* P) { return noalloc_spec_offset(P) + P->F_bytes(); }
+size_t noalloc_scale_offset(const hpx_plan_s* P) {
+    return noalloc_spec_offset(P) + ((P->F_bytes() + 255) & ~(size_t)255);
+}
+size_t noalloc_need(const hpx_plan_s* P) { return noalloc_scale_offset(P) + P->scale_bytes(); }
 
 }  // namespace
 
@@ -726,7 +762,7 @@ int noalloc_scratch(int device, unsigned char** out) {
 template <typename T>
 int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch, unsigned char* scratch,
                         cudaStream_t st) {
-    Pipeline<T> pl(P, (T*)scratch, (T*)(scratch + noalloc_spec_offset(P)), st);
+    Pipeline<T> pl(P, (T*)scratch, (T*)(scratch + noalloc_spec_offset(P)), (char*)scratch + noalloc_scale_offset(P), st);
     const int64_t bc = P->batch_chunk;
     const size_t alm_stride = (size_t)P->L * P->M * 2;
     for (int64_t b0 = 0; b0 < batch; b0 += bc) {
@@ -775,7 +811,7 @@ int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan) {
     if (desc->nside < 1 || desc->nside > 8192) return set_err(HPX_ERR_INVALID_ARG, "nside must be in [1, 8192]");
     if (desc->lmax < 1 || desc->mmax < 1) return set_err(HPX_ERR_INVALID_ARG, "lmax and mmax must be >= 1");
     if (desc->lmax > 65536 || desc->mmax > 65536) return set_err(HPX_ERR_INVALID_ARG, "lmax/mmax too large");
-    if (desc->precision < HPX_PREC_FP32 || desc->precision > HPX_PREC_TF32)
+    if (desc->precision < HPX_PREC_FP32 || desc->precision > HPX_PREC_F16X3)
         return set_err(HPX_ERR_INVALID_ARG, "unknown precision");
     if (desc->batch_chunk < 0 || desc->batch_chunk > 4096) return set_err(HPX_ERR_INVALID_ARG, "batch_chunk out of range");
     if (desc->refine_iters < 0 || desc->refine_iters > 64) return set_err(HPX_ERR_INVALID_ARG, "refine_iters out of range");
@@ -818,6 +854,7 @@ int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
                ((plan->resid_bytes() + 255) & ~(size_t)255);
     s += (plan->tcA_bytes() + 255) & ~(size_t)255;
     s += (plan->F_bytes() + 255) & ~(size_t)255;
+    s += plan->scale_bytes();
     *bytes = s;
     return HPX_OK;
 }

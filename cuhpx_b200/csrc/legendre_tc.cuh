@@ -1,4 +1,4 @@
-// Tensor-core (tcgen05) Legendre contraction, BF16 3-term split, FP32 accumulate.
+// Tensor-core (tcgen05) Legendre contraction, BF16 or FP16 3-term split, FP32 accumulate.
 //
 // Same mathematics as the SIMT kernels in legendre.cuh (orthonormal Pbar_l^m,
 // north/south folding, per-m contraction), mapped onto the 5th-generation
@@ -13,10 +13,19 @@
 //    synthesis) is pre-split into bf16 hi/lo in global memory and brought in by
 //    TMA (cp.async.bulk.tensor, 128B swizzle, no multicast);
 //  * one thread issues tcgen05.mma (M=128, N=128, K=16) for the three products
-//    hi*hi + hi*lo + lo*hi into FP32 accumulators in TMEM; tcgen05.commit
-//    frees a pipeline stage when its MMAs retire;
-//  * four epilogue warps drain TMEM (tcgen05.ld) while the next tile
-//    accumulates into the other half of TMEM.
+//    into FP32 accumulators in TMEM; tcgen05.commit frees a pipeline stage
+//    when its MMAs retire;
+//  * four epilogue warps drain TMEM (tcgen05.ld) and add the accumulators.
+//
+// TMEM (512 columns) holds, per parity, a main accumulator (hi*hi) and a cross
+// accumulator (hi*lo + lo*hi), at column (2 par + part) * 128.  The tensor
+// cores' FP32 accumulation rounds toward zero at every MMA (an MMA adding
+// 0.99 ulp to 1.0 leaves it unchanged), so each MMA into an accumulator can
+// lose up to one ulp of its magnitude, always in the same direction; the bias
+// grows with the number of MMAs chained into it.  Keeping the cross products,
+// 2^-8 (bf16) or 2^-11 (fp16) smaller, in their own accumulator leaves one MMA
+// per K-step on the main one, and the epilogue adds the two with
+// round-to-nearest FP32.
 //
 // Analysis tile  = (m, 256 consecutive degrees): D_par[128 l][128 cols] +=
 //                   Pbar_par[128 l][32 rings] * X_par[32 rings][128 cols]
@@ -98,11 +107,39 @@ __device__ __forceinline__ uint32_t split_pair(float fa, float fb, uint32_t& lo)
     lo = *(const uint32_t*)&l;
     return hb;
 }
+// the same with fp16 halves: hi = f16_rn(x), lo = f16_rn(x - hi)
+__device__ __forceinline__ uint32_t split_pair_h(float fa, float fb, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(fa, fb);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(fa - hf.x, fb - hf.y);
+    lo = *(const uint32_t*)&l;
+    return *(const uint32_t*)&h;
+}
+template <bool F16>
 __device__ __forceinline__ void split8f(const float* v, uint4& hi, uint4& lo) {
-    hi.x = split_pair(v[0], v[1], lo.x);
-    hi.y = split_pair(v[2], v[3], lo.y);
-    hi.z = split_pair(v[4], v[5], lo.z);
-    hi.w = split_pair(v[6], v[7], lo.w);
+    if constexpr (F16) {
+        hi.x = split_pair_h(v[0], v[1], lo.x);
+        hi.y = split_pair_h(v[2], v[3], lo.y);
+        hi.z = split_pair_h(v[4], v[5], lo.z);
+        hi.w = split_pair_h(v[6], v[7], lo.w);
+    } else {
+        hi.x = split_pair(v[0], v[1], lo.x);
+        hi.y = split_pair(v[2], v[3], lo.y);
+        hi.z = split_pair(v[4], v[5], lo.z);
+        hi.w = split_pair(v[6], v[7], lo.w);
+    }
+}
+
+// 1 / 2^e(map) of the FP16 operand scale for the first kTcCols/2 maps (1 for BF16)
+template <bool F16>
+__device__ __forceinline__ void load_inv_scales(float* s_inv, const unsigned* __restrict__ vmax, float bound_mul,
+                                                int nmaps) {
+    const int b = threadIdx.x;
+    if (b < kTcCols / 2) {
+        float v = 1.f;
+        if (F16 && b < nmaps) v = tc::pow2f(-tc::f16_scale_exp(__uint_as_float(vmax[b]) * bound_mul));
+        s_inv[b] = v;
+    }
 }
 
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
@@ -231,12 +268,15 @@ __device__ __forceinline__ void gen1_slow(int chain, int m, int l0b, int L, int 
 // producer groups than stages an mbarrier parity wait could pass on a stale
 // phase).  Lane = (ring r = lane&15, block pair bp = lane>>4) runs the two
 // blocks 2bp, 2bp+1 of its ring.
+template <bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map, int nmaps,
                  float* __restrict__ alm, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
                  const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
                  const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
-                 const int2* __restrict__ tiles, int ntiles, int accumulate, int* __restrict__ err) {
+                 const int2* __restrict__ tiles, int ntiles, int accumulate, const unsigned* __restrict__ fmax,
+                 float wb, int* __restrict__ err) {
+    __shared__ float s_inv[kTcCols / 2];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // align by pointer arithmetic on the shared array (keeps the shared address space known)
     unsigned char* base = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -246,6 +286,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = 2 * nside;
     const int nbk = seed_blocks(L);
+    load_inv_scales<F16>(s_inv, fmax, wb, nmaps);
     tc_setup(sh, kFStages, 1, warp);
     const uint32_t tmem = sh->tmem_base;
     auto nchunks = [&](int m) { return (NP - first_ring_for_m(m, nside) + kFRing - 1) / kFRing; };
@@ -281,17 +322,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16(128, kTcCols, true, true);
+            const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, true, true) : tc::idesc_bf16(128, kTcCols, true, true);
             int it = 0, tcount = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
-                const int a = tcount & 1;
                 TCP_T0(w2);
-                if (!tc::mbar_wait(&sh->acc_empty[a], ((tcount >> 1) & 1) ^ 1, err, 12)) break;
+                if (!tc::mbar_wait(&sh->acc_empty[0], (tcount & 1) ^ 1, err, 12)) break;
                 TCP_ADD(0, 2, w2);
                 tc::tc_fence_after();
-                const uint32_t dbase = tmem + a * 2 * kTcCols;
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kFStages;
                     const uint32_t ph = (it / kFStages) & 1;
@@ -306,18 +345,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const uint32_t sb = sa + 16384;
 #pragma unroll
                     for (int par = 0; par < 2; ++par) {
-                        const uint32_t d = dbase + par * kTcCols;
+                        const uint32_t dm = tmem + par * 2 * kTcCols, dc = dm + kTcCols;
                         const uint64_t ah = tc::smem_desc_sw128(sa + (par * 2 + 0) * 4096, 2048, 1024);
                         const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * 4096, 2048, 1024);
                         const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 4096, 2048, 1024);
                         const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 4096, 2048, 1024);
-                        tc::mma_bf16(d, ah, bh, idesc, c > 0 ? 1u : 0u);
-                        tc::mma_bf16(d, ah, bl, idesc, 1u);
-                        tc::mma_bf16(d, al, bh, idesc, 1u);
+                        tc::mma_bf16(dm, ah, bh, idesc, c > 0 ? 1u : 0u);
+                        tc::mma_bf16(dc, ah, bl, idesc, c > 0 ? 1u : 0u);
+                        tc::mma_bf16(dc, al, bh, idesc, 1u);
                     }
                     tc::mma_commit(&sh->empty[s]);
                 }
-                tc::mma_commit(&sh->acc_full[a]);
+                tc::mma_commit(&sh->acc_full[0]);
             }
         mma_done:
             mma_drain(sh);
@@ -329,7 +368,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
             const int m = tiles[t].x, jb = tiles[t].y;
             const int l0 = m + jb * kTcFwdDeg;
-            const int a = tcount & 1;
             // zero the l < m triangle of this column while the tile accumulates
             if (!accumulate && jb == 0) {
                 const int nz = min(m, L);
@@ -339,7 +377,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             }
             TCP_T0(e0);
-            if (!tc::mbar_wait_warp(&sh->acc_full[a], (tcount >> 1) & 1, err, 15)) break;
+            if (!tc::mbar_wait_warp(&sh->acc_full[0], tcount & 1, err, 15)) break;
             if (lane == 0) TCP_ADD(0, 5, e0);
             TCP_T0(e1);
             tc::tc_fence_after();
@@ -347,18 +385,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll 1
             for (int par = 0; par < 2; ++par) {
                 const int l = l0 + 2 * row + par;
-                const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + a * 2 * kTcCols + par * kTcCols;
+                const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + par * 2 * kTcCols;
 #pragma unroll 1
                 for (int c = 0; c < kTcCols; c += 16) {
-                    float v[16];
+                    float v[16], w[16];
                     tc::tmem_ld16(taddr + c, v);
+                    tc::tmem_ld16(taddr + kTcCols + c, w);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] += w[j];
                     if (l < L) {
 #pragma unroll
                         for (int j = 0; j < 16; j += 2) {
                             const int b = (c + j) >> 1;
                             if (b < nmaps) {
                                 float2* dst = (float2*)(alm + 2 * (((int64_t)b * L + l) * M + m));
-                                float2 o = make_float2(v[j], v[j + 1]);
+                                const float sb = s_inv[b];
+                                float2 o = make_float2(v[j] * sb, v[j + 1] * sb);
                                 if (accumulate) {
                                     const float2 q = *dst;
                                     o.x += q.x;
@@ -372,7 +414,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             tc::tc_fence_before();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&sh->acc_empty[a]);
+            if (lane == 0) tc::mbar_arrive(&sh->acc_empty[0]);
             if (lane == 0) TCP_ADD(0, 6, e1);
         }
     } else if (warp >= 8 && warp < 8 + kFStages) {
@@ -448,8 +490,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 auto emit = [&](int chain, int sidx, const float* ev, const float* od) {
                     const int q = 2 * bp + chain;  // 64-degree block within the tile
                     uint4 eh, el, oh, ol;
-                    split8f(ev, eh, el);
-                    split8f(od, oh, ol);
+                    split8f<F16>(ev, eh, el);
+                    split8f<F16>(od, oh, ol);
                     const uint32_t off = (uint32_t)((q >> 1) * 2048) + gbase + tc::sw128_offset(r & 7, ((q & 1) << 2) + sidx);
                     st_shared_v4(sa + 0 * 4096 + off, eh);
                     st_shared_v4(sa + 1 * 4096 + off, el);
@@ -500,12 +542,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // Chunk it goes to producer pair g = it mod 3 (warps 8+2g, 9+2g), which owns
 // stage g (one barrier phase of run-ahead at most); lane runs rings 32w + lane
 // and 64 + 32w + lane of the tile.
+template <bool F16>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_inv_tc(const __grid_constant__ CUtensorMap ah_map, const __grid_constant__ CUtensorMap al_map,
-                 float* __restrict__ spec, int C, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
-                 const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
-                 const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
-                 const int2* __restrict__ tiles, int ntiles, int* __restrict__ err) {
+                 float* __restrict__ spec, int C, int nmaps, int L, int M, int Lpad, int nside,
+                 const double* __restrict__ zr, const int* __restrict__ lstart, const int* __restrict__ lsmax,
+                 const double2* __restrict__ pstart, const double2* __restrict__ coef,
+                 const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds, const int2* __restrict__ tiles,
+                 int ntiles, const unsigned* __restrict__ amax, int* __restrict__ err) {
+    __shared__ float s_inv[kTcCols / 2];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // align by pointer arithmetic on the shared array (keeps the shared address space known)
     unsigned char* base = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -515,6 +560,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = 2 * nside;
     const int nbk = seed_blocks(L);
+    load_inv_scales<F16>(s_inv, amax, 1.f, nmaps);
     tc_setup(sh, kIStages, 2, warp);
     const uint32_t tmem = sh->tmem_base;
     auto nchunks = [&](int m) { return m < L ? (L - m + kTcDegChunk - 1) / kTcDegChunk : 0; };
@@ -548,17 +594,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16(128, kTcCols, false, true);
+            const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, false, true) : tc::idesc_bf16(128, kTcCols, false, true);
             int it = 0, tcount = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
-                const int a = tcount & 1;
                 TCP_T0(w2);
-                if (!tc::mbar_wait(&sh->acc_empty[a], ((tcount >> 1) & 1) ^ 1, err, 22)) break;
+                if (!tc::mbar_wait(&sh->acc_empty[0], (tcount & 1) ^ 1, err, 22)) break;
                 TCP_ADD(1, 2, w2);
                 tc::tc_fence_after();
-                const uint32_t dbase = tmem + a * 2 * kTcCols;
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kIStages;
                     const uint32_t ph = (it / kIStages) & 1;
@@ -573,21 +617,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const uint32_t sb = sa + 32768;
 #pragma unroll
                     for (int par = 0; par < 2; ++par) {
-                        const uint32_t d = dbase + par * kTcCols;
+                        const uint32_t dm = tmem + par * 2 * kTcCols, dc = dm + kTcCols;
 #pragma unroll
                         for (int ks = 0; ks < 2; ++ks) {
                             const uint64_t ah = tc::smem_desc_kmajor_sw64(sa + (par * 2 + 0) * 8192 + ks * 32, 512);
                             const uint64_t al = tc::smem_desc_kmajor_sw64(sa + (par * 2 + 1) * 8192 + ks * 32, 512);
                             const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 8192 + ks * 2048, 4096, 1024);
                             const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 8192 + ks * 2048, 4096, 1024);
-                            tc::mma_bf16(d, ah, bh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-                            tc::mma_bf16(d, ah, bl, idesc, 1u);
-                            tc::mma_bf16(d, al, bh, idesc, 1u);
+                            const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+                            tc::mma_bf16(dm, ah, bh, idesc, acc);
+                            tc::mma_bf16(dc, ah, bl, idesc, acc);
+                            tc::mma_bf16(dc, al, bh, idesc, 1u);
                         }
                     }
                     tc::mma_commit(&sh->empty[s]);
                 }
-                tc::mma_commit(&sh->acc_full[a]);
+                tc::mma_commit(&sh->acc_full[0]);
             }
         mma_done:
             mma_drain(sh);
@@ -599,28 +644,33 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
             const int m = tiles[t].x, rb = tiles[t].y;
             const int t0 = first_ring_for_m(m, nside);
-            const int a = tcount & 1;
             const int rr = rb + ew * 32 + lane;
             const int p = t0 + rr;
-            if (!tc::mbar_wait_warp(&sh->acc_full[a], (tcount >> 1) & 1, err, 25)) break;
+            if (!tc::mbar_wait_warp(&sh->acc_full[0], tcount & 1, err, 25)) break;
             tc::tc_fence_after();
 #pragma unroll 1
             for (int par = 0; par < 2; ++par) {
                 float* dst = spec + (((int64_t)m * 2 + par) * NP + p) * C;
-                const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + a * 2 * kTcCols + par * kTcCols;
+                const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + par * 2 * kTcCols;
 #pragma unroll 1
                 for (int c = 0; c < kTcCols; c += 16) {
-                    float v[16];
+                    float v[16], w[16];
                     tc::tmem_ld16(taddr + c, v);
+                    tc::tmem_ld16(taddr + kTcCols + c, w);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] += w[j];
                     if (p < NP && c < C) {
 #pragma unroll
-                        for (int j = 0; j < 16; j += 4) *(float4*)(dst + c + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                        for (int j = 0; j < 16; j += 4) {
+                            const float s0 = s_inv[(c + j) >> 1], s1 = s_inv[((c + j) >> 1) + 1];
+                            *(float4*)(dst + c + j) = make_float4(v[j] * s0, v[j + 1] * s0, v[j + 2] * s1, v[j + 3] * s1);
+                        }
                     }
                 }
             }
             tc::tc_fence_before();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&sh->acc_empty[a]);
+            if (lane == 0) tc::mbar_arrive(&sh->acc_empty[0]);
         }
     } else if (warp >= 8 && warp < 8 + 2 * kIStages) {
         // ------------------------------------------------ Pbar^T producers
@@ -694,8 +744,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 auto emit = [&](int chain, int sidx, const float* ev, const float* od) {
                     const int rr = chain ? r1 : r0;
                     uint4 eh, el, oh, ol;
-                    split8f(ev, eh, el);
-                    split8f(od, oh, ol);
+                    split8f<F16>(ev, eh, el);
+                    split8f<F16>(od, oh, ol);
                     const uint32_t off = (uint32_t)((rr >> 3) * 512) + tc::sw64_offset(rr & 7, sidx);
                     st_shared_v4(sa + 0 * 8192 + off, eh);
                     st_shared_v4(sa + 1 * 8192 + off, el);
@@ -740,8 +790,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ================================================================== operand preparation
 // alm[b][l][m] (FP32 complex) -> Ah/Al bf16 [2M][Lh][128]: row i of (m, par) is
 // degree l = m + 2i + par; rows with l >= L (up to L+63) are written as zeros.
+// amax != nullptr: fp16 halves of the values times 2^e(map), e from the map's
+// max |a| (k_rows_maxabs); otherwise bf16 halves.
 __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int M, int Lh,
-                            uint16_t* __restrict__ ah, uint16_t* __restrict__ al) {
+                            uint16_t* __restrict__ ah, uint16_t* __restrict__ al, const unsigned* __restrict__ amax) {
     __shared__ float2 tile[64][33];
     const int m0 = blockIdx.x * 32, l = blockIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
@@ -763,8 +815,14 @@ __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int
         for (int b = tx; b < 64; b += 32) {
             const float2 v = tile[b][mi];
             uint16_t h0, l0, h1, l1;
-            tc::split_bf16(v.x, h0, l0);
-            tc::split_bf16(v.y, h1, l1);
+            if (amax) {
+                const float sc = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? amax[b] : 0u)));
+                tc::split_f16(v.x * sc, h0, l0);
+                tc::split_f16(v.y * sc, h1, l1);
+            } else {
+                tc::split_bf16(v.x, h0, l0);
+                tc::split_bf16(v.y, h1, l1);
+            }
             rh[b] = pack_bf16x2(h0, h1);
             rl[b] = pack_bf16x2(l0, l1);
         }

@@ -261,8 +261,9 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
 }
 
 // Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
+// Returns the largest |re|, |im| this thread wrote.
 template <typename T>
-__device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ F,
+__device__ T ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ F,
                              const RingPair& rp, const cplx<T>* __restrict__ twP, const cplx<T>* __restrict__ gtab,
                              const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g) {
     const int h = rp.h;
@@ -270,6 +271,7 @@ __device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, c
         buf[padi(j)] = *(const cplx<T>*)(x + 2 * j);
     }
     cplx<T>* Z = ring_dft(buf, buf2, rp, twP, gtab, chirp, false, lt, tpf, g);
+    T mx = (T)0;
     for (int k = lt; k < rp.mt; k += tpf) {
         const int k1 = k == h ? 0 : k;
         const int k2 = k == 0 ? 0 : h - k;
@@ -281,8 +283,10 @@ __device__ void ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, c
         cplx<T> X = cadd(Ek, cmul(E(2 * k), Ok));
         if (shift) X = cmul(E(k), X);
         *(cplx<T>*)(F + 2 * k) = X;
+        mx = fmax(mx, fmax(fabs(X.re), fabs(X.im)));
     }
     group_sync(tpf, g);
+    return mx;
 }
 
 // Inverse transform of the ring spectrum Fg[0..mt) (global) into one real ring

@@ -11,6 +11,7 @@
 
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -155,6 +156,15 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn, bool 
            | ((uint32_t)(M >> 4) << 24);  // M
 }
 
+// Instruction descriptor for kind::f16 with FP16 A/B (format code 0), FP32 accumulate.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool a_mn, bool b_mn) {
+    return (1u << 4)                      // D format F32
+           | ((a_mn ? 1u : 0u) << 15)     // A major
+           | ((b_mn ? 1u : 0u) << 16)     // B major
+           | ((uint32_t)(N >> 3) << 17)   // N
+           | ((uint32_t)(M >> 4) << 24);  // M
+}
+
 // D[tmem] (+)= A[smem] * B[smem]; issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -191,6 +201,31 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) 
     hi = __bfloat16_as_ushort(h);
     lo = __bfloat16_as_ushort(l);
 }
+
+// ---------------------------------------------------------------- fp16 split
+// x = hi + lo with hi = f16(x) and lo = f16(x - hi): about 22 significant bits
+// for |x| in [2^-3, 2^15]; below that lo is subnormal and the absolute error
+// stays under 2^-25.
+__device__ __forceinline__ void split_f16(float x, uint16_t& hi, uint16_t& lo) {
+    const __half h = __float2half_rn(x);
+    const __half l = __float2half_rn(x - __half2float(h));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+}
+
+// Power-of-two scale of the FP16 operands of one map: e such that a bound B
+// on the map's operand magnitudes maps below 2^14 (fp16 max is 65504), so
+// every value keeps 22 bits down to 2^-17 of the bound.  0, inf and NaN
+// bounds give e = 0.
+__device__ __forceinline__ int f16_scale_exp(float bound) {
+    if (!(bound > 0.f) || !(bound < 3.0e38f)) return 0;
+    int ex = 0;
+    (void)frexpf(bound, &ex);  // bound < 2^ex
+    const int e = 14 - ex;
+    return e < -120 ? -120 : (e > 120 ? 120 : e);
+}
+// 2^e for |e| <= 126, exactly
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
 
 // Byte offset of the 16-byte chunk `chunk` (0..7) of row `row` inside a
 // SWIZZLE_128B atom (8 rows x 128 bytes), the pattern TMA and UMMA share.

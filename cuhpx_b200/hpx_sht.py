@@ -19,8 +19,9 @@ Differences from the reference, all deliberate:
   pins the stream that was current at construction);
 * gradients are the exact adjoints of the transforms (the reference's
   hand-written backward is approximate, cuhpx/hpx_sht.py:565-583, 614-641);
-* keyword-only extras: ``precision`` ('fp32' or 'bf16x3': tcgen05 tensor
-  cores with a three-term bf16 split and FP32 accumulation),
+* keyword-only extras: ``precision`` ('fp32'; 'f16x3' or 'bf16x3': tcgen05
+  tensor cores with a three-term fp16 (per-map power-of-two scaled, ~22-bit)
+  or bf16 (~16-bit) split and FP32 accumulation),
   ``refine_iters`` (Jacobi refinement of the analysis), ``batch_chunk``.
 """
 
@@ -230,8 +231,8 @@ class _Base(nn.Module):
         self.quad_weights = quad_weights
         self.lmax = lmax or self.nlat
         self.mmax = mmax or (self.nlon // 2 + 1)
-        if precision not in ("fp32", "bf16x3"):
-            raise ValueError("precision must be 'fp32' or 'bf16x3' (float64 data select fp64 automatically)")
+        if precision not in ("fp32", "bf16x3", "f16x3"):
+            raise ValueError("precision must be 'fp32', 'f16x3' or 'bf16x3' (float64 data select fp64 automatically)")
         self.precision = precision
         self.refine_iters = int(refine_iters)
         self.batch_chunk = int(batch_chunk)

@@ -52,12 +52,16 @@ typedef enum {
 } hpx_status_t;
 
 /* Arithmetic of the Legendre contraction.  FFT stages run in float for
- * FP32/BF16X3/TF32 plans and in double for FP64 plans. */
+ * FP32/BF16X3/F16X3/TF32 plans and in double for FP64 plans. */
 typedef enum {
     HPX_PREC_FP32 = 0,   /* FP32 SIMT contraction ("plain FP32 path") */
     HPX_PREC_FP64 = 1,   /* FP64 everywhere (double I/O)              */
-    HPX_PREC_BF16X3 = 2, /* tcgen05 BF16 3-term split, FP32 accumulate */
-    HPX_PREC_TF32 = 3    /* tcgen05 TF32, FP32 accumulate             */
+    HPX_PREC_BF16X3 = 2, /* tcgen05 BF16 3-term split (hi*hi + hi*lo + lo*hi),
+                            FP32 accumulate; ~16-bit operands          */
+    HPX_PREC_TF32 = 3,   /* tcgen05 TF32, FP32 accumulate (not built)  */
+    HPX_PREC_F16X3 = 4   /* tcgen05 FP16 3-term split with a power-of-two
+                            scale per map, FP32 accumulate; ~22-bit
+                            operands, same speed as BF16X3             */
 } hpx_precision_t;
 
 typedef struct {
@@ -116,7 +120,7 @@ HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void*
  * of one chunk of batch_chunk maps kept in one static device array of
  * 32 MiB (33554432 bytes) per device, shared by every plan and call on that
  * device.  A plan whose chunk needs more (per chunk of 64 maps: about 28 MiB at
- * nside 64, lmax = mmax = 128 for FP32/BF16X3; FP64 twice that) is refused with
+ * nside 64, lmax = mmax = 128 for FP32/BF16X3/F16X3; FP64 twice that) is refused with
  * HPX_ERR_WORKSPACE before anything runs.  Nothing in the array has to start
  * at zero.  Calls that overlap in time -- on two streams, or from two threads --
  * race on the array and give wrong results: serialise them.  The first call on

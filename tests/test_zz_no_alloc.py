@@ -48,13 +48,14 @@ def forward_ws(lib, plan, f, alm, stream):
     _lib.check(lib.hpx_sht_forward(plan, f.data_ptr(), alm.data_ptr(), f.shape[0], base, need.value, stream), plan)
 
 
-# (nside, L, M, precision, batch): FP32, BF16X3 and FP64 plans; batches of one
+# (nside, L, M, precision, batch): FP32, BF16X3, F16X3 and FP64 plans; batches of one
 # chunk, a partial chunk and two chunks (the second one partial)
 CASES = [
     (16, 33, 33, 0, 5),
     (32, 64, 64, 0, 64),
     (32, 65, 65, 2, 70),
     (64, 128, 128, 2, 64),
+    (32, 65, 65, 4, 70),
     (16, 33, 33, 1, 3),
     (32, 64, 64, 1, 66),
 ]
