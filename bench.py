@@ -424,6 +424,14 @@ def algorithmic(nside, L, M):
     return flops, fft_bytes
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per full launch of the
+# dominant kernel, from one single-pass ncu capture of this script's default
+# workload: (stage, nside, lmax, precision) -> bytes
+MEASURED_TRAFFIC = {
+    ("legendre_forward", 1024, 2047, "f16x3"): 14.94e9 + 6.84e9,
+}
+
+
 def roofline(stats, args, prec, refine, nside, L, B):
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
@@ -439,6 +447,7 @@ def roofline(stats, args, prec, refine, nside, L, B):
             # fp16 and bf16 run at the same tcgen05 kind::f16 rate
             peak = peaks.get("bf16_tflops", 1590.0) if prec != "tf32" else peaks.get("bf16_tflops", 1590.0) / 2
             achieved = useful * terms / (per_launch_ms * 1e-3) / 1e12
+            traffic = MEASURED_TRAFFIC.get((name, nside, L, prec)) if B >= 64 else None
             return {
                 "kernel": name,
                 "bound": "tensor",
@@ -446,7 +455,8 @@ def roofline(stats, args, prec, refine, nside, L, B):
                 "peak": peak,
                 "unit": "TFLOP/s",
                 "frac": achieved / peak,
-                "traffic": None,
+                "traffic": traffic,
+                "traffic_unit": "bytes per launch",
                 "useful_tflops": useful / (per_launch_ms * 1e-3) / 1e12,
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" + ("; tf32 taken as half" if prec == "tf32" else ""),
             }
@@ -460,7 +470,7 @@ def roofline(stats, args, prec, refine, nside, L, B):
             "unit": "TFLOP/s",
             "frac": achieved / peak,
             "traffic": None,
-            "peak_source": "FMA-loop peak measured on this pool's B200 (profiles/peaks_fp32_fp64.md)",
+            "peak_source": "nominal FP32 FMA rate: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz",
         }
     byts = fft_bytes_map * chunk
     achieved = byts / (per_launch_ms * 1e-3) / 1e9
@@ -468,8 +478,8 @@ def roofline(stats, args, prec, refine, nside, L, B):
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None}
 
 
-# measured with an FMA loop on this pool's B200 (see profiles/peaks_fp32_fp64.md)
-FP32_SIMT_PEAK_TFLOPS = 72.0
+# FP32 CUDA-core peak of a B200 at its maximum SM clock
+FP32_SIMT_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def main():
