@@ -102,6 +102,7 @@ struct hpx_plan_s {
     double* d_z = nullptr;       // cos(theta) of the north rings
     AlphaC* d_alphac = nullptr;  // [M][Lpad] block-normalised recurrence (tensor-core producers)
     int* d_lsmax = nullptr;      // per order: max over its rings of the first significant degree
+    std::vector<int> h_lsmax;
     int n_fwdtiles = 0;
     float wmax = 0.f;            // largest ring weight w_t
     size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
@@ -150,6 +151,8 @@ struct hpx_plan_s {
         cudaFree(tc.d_err);
         cudaFree(tc.d_fwd_tiles);
         cudaFree(tc.d_inv_tiles);
+        cudaFree(tc.d_fwd_off);
+        cudaFree(tc.d_inv_off);
         for (auto& r : stats_recs) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
@@ -237,6 +240,33 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+// Assignment of tiles to at most `nsm` CTAs: tiles sorted by decreasing cost
+// (ties in list order, so a round holds neighbouring orders and CTAs working
+// at the same time share each order's data operand in L2) are dealt out in
+// rounds of one tile per CTA, alternating direction each round, which evens
+// the CTAs' sums.  Returns the CTA count; `order` receives the tiles grouped by
+// CTA (each in round order) and `off` the CTA boundaries.
+int schedule_tiles(const std::vector<int2>& tiles, const std::vector<double>& cost, int nsm, std::vector<int2>& order,
+                   std::vector<int>& off) {
+    const int n = (int)tiles.size();
+    const int nc = std::max(1, std::min(nsm, n));
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<std::vector<int>> per(nc);
+    for (int k = 0; k < n; ++k) {
+        const int round = k / nc, pos = k % nc;
+        per[(round & 1) ? nc - 1 - pos : pos].push_back(idx[k]);
+    }
+    order.clear();
+    off.assign(1, 0);
+    for (auto& v : per) {
+        for (int i : v) order.push_back(tiles[i]);
+        off.push_back((int)order.size());
+    }
+    return nc;
+}
+
 // Tensor-core plan: tile lists, error flag, tensor-map encoder.
 int tc_create(hpx_plan_s* P) {
     TcPlan& T = P->tc;
@@ -261,13 +291,36 @@ int tc_create(hpx_plan_s* P) {
     }
     T.n_fwd_tiles = (int)ft.size();
     T.n_inv_tiles = (int)it.size();
+    // Tile costs in producer chunks: a chunk whose degrees start below the
+    // order's largest first significant degree takes the slower
+    // start-injecting recurrence (about twice the time); every tile also pays
+    // a fixed epilogue of about seven chunks.
+    constexpr double kSlow = 2.0, kTileFixed = 7.0;
+    std::vector<double> fc, ic;
+    for (const int2& t : ft) {
+        const int nch = (P->NP - first_ring_for_m(t.x, N) + kFRing - 1) / kFRing;
+        fc.push_back(nch * (t.x + t.y * kTcFwdDeg < P->h_lsmax[t.x] ? kSlow : 1.0) + kTileFixed);
+    }
+    for (const int2& t : it) {
+        double c = kTileFixed;
+        for (int l0 = t.x; l0 < P->L; l0 += kTcDegChunk) c += l0 < P->h_lsmax[t.x] ? kSlow : 1.0;
+        ic.push_back(c);
+    }
+    std::vector<int2> order;
+    std::vector<int> off;
     if (!ft.empty()) {
-        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_tiles, sizeof(int2) * ft.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_tiles, ft.data(), sizeof(int2) * ft.size(), cudaMemcpyHostToDevice));
+        T.n_fwd_ctas = schedule_tiles(ft, fc, T.nsm, order, off);
+        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_tiles, sizeof(int2) * order.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_off, sizeof(int) * off.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
     }
     if (!it.empty()) {
-        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * it.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, it.data(), sizeof(int2) * it.size(), cudaMemcpyHostToDevice));
+        T.n_inv_ctas = schedule_tiles(it, ic, T.nsm, order, off);
+        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * order.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_off, sizeof(int) * off.size()));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
     }
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
@@ -406,6 +459,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
             for (int p = t0; p < P->NP; ++p) mx = std::max(mx, hls[(size_t)m * P->NP + p]);
             hmax[m] = mx;
         }
+        P->h_lsmax = hmax;
         HPX_CUDA_TRY(cudaMalloc(&P->d_lsmax, sizeof(int) * P->M));
         HPX_CUDA_TRY(cudaMemcpy(P->d_lsmax, hmax.data(), sizeof(int) * P->M, cudaMemcpyHostToDevice));
     }
@@ -595,9 +649,9 @@ struct Pipeline {
             if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
             auto kern = P->f16() ? k_leg_fwd_tc<true> : k_leg_fwd_tc<false>;
-            kern<<<std::min(TP.n_fwd_tiles, TP.nsm), kTcThreads, kFSmem, st>>>(
+            kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(
                 mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
-                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.n_fwd_tiles, accumulate, fmax,
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, accumulate, fmax,
                 fold_wb, TP.d_err);
             return;
         }
@@ -633,9 +687,9 @@ struct Pipeline {
             if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
             auto kern = P->f16() ? k_leg_inv_tc<true> : k_leg_inv_tc<false>;
-            kern<<<std::min(TP.n_inv_tiles, TP.nsm), kTcThreads, kISmem, st>>>(
+            kern<<<TP.n_inv_ctas, kTcThreads, kISmem, st>>>(
                 mh, ml, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
-                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.n_inv_tiles, amax, TP.d_err);
+                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.d_inv_off, amax, TP.d_err);
             return;
         }
         dim3 tg((P->M + 31) / 32, P->L, (nb + 15) / 16);
@@ -967,7 +1021,7 @@ const char* hpx_status_string(int status) {
 // Instrumented builds only: copy and clear the per-CTA role timers.
 extern "C" HPX_API int hpx_tc_profile_read(unsigned long long* out) {
     cudaMemcpyFromSymbol(out, g_tc_prof, sizeof(g_tc_prof));
-    static unsigned long long zero[2][296][8];
+    static unsigned long long zero[2][296][kTcpSlots];
     cudaMemcpyToSymbol(g_tc_prof, zero, sizeof(g_tc_prof));
     return HPX_OK;
 }

@@ -33,7 +33,8 @@
 //                   Pbar^T[128 rings][32 l] * A_par[32 l][128 cols]
 // where par is the parity of l-m and cols = 2*map + {re, im}.
 //
-// Persistent kernels, one CTA per SM, static round-robin over a tile list.
+// Persistent kernels, one CTA per SM; each CTA runs its own contiguous range of
+// the plan's tile list (tile_off[cta] .. tile_off[cta+1]), balanced on the host.
 // Every mbarrier wait is bounded (tc_ptx.cuh); a timeout writes an error code
 // to the plan's device flag and the kernel drains and returns.
 #pragma once
@@ -44,14 +45,31 @@
 namespace hpx {
 
 // Optional per-CTA role timers (built only with -DHPX_TC_PROFILE): cycles each
-// role spends waiting vs working, read back by hpx_tc_profile_read.
+// role spends waiting vs working, summed in registers and added to
+// g_tc_prof once when the role finishes (so no global atomic sits between a
+// role's stores and its release-arrive), read back by hpx_tc_profile_read.
+// Slots: 0-2 MMA waits (TMA data, producers, accumulator free); 3 producer
+// wait for a free stage, 4 producer work (wait end to arrive), 7 recurrence,
+// 8 producer loop between chunks, 9 proxy fence + arrive; 5-6 epilogue wait
+// and work; 10 the MMA thread's whole run.
 #ifdef HPX_TC_PROFILE
-__device__ unsigned long long g_tc_prof[2][148 * 2][8];
+constexpr int kTcpSlots = 16;
+__device__ unsigned long long g_tc_prof[2][148 * 2][kTcpSlots];
+#define TCP_DECL unsigned long long tcp_acc[kTcpSlots] = {}
 #define TCP_T0(v) long long v = clock64()
-#define TCP_ADD(k, slot, v) atomicAdd(&g_tc_prof[k][blockIdx.x % 296][slot], (unsigned long long)(clock64() - (v)))
+#define TCP_SET(v) v = clock64()
+#define TCP_ADD(k, slot, v) (tcp_acc[slot] += (unsigned long long)(clock64() - (v)))
+#define TCP_FLUSH(k)                                                                          \
+    do {                                                                                      \
+        _Pragma("unroll") for (int i_ = 0; i_ < kTcpSlots; ++i_) if (tcp_acc[i_])             \
+            atomicAdd(&g_tc_prof[k][blockIdx.x % 296][i_], tcp_acc[i_]);                      \
+    } while (0)
 #else
+#define TCP_DECL
 #define TCP_T0(v)
+#define TCP_SET(v)
 #define TCP_ADD(k, slot, v)
+#define TCP_FLUSH(k)
 #endif
 
 constexpr int kTcCols = 128;      // N: columns per tile (64 maps)
@@ -76,10 +94,12 @@ struct TcPlan {
     int active = 0;
     int nsm = 0;
     int* d_err = nullptr;     // device error flag written by bounded waits
-    int2* d_fwd_tiles = nullptr;
-    int n_fwd_tiles = 0;
+    int2* d_fwd_tiles = nullptr;  // tiles grouped by CTA
+    int* d_fwd_off = nullptr;     // CTA c runs tiles d_fwd_off[c] .. d_fwd_off[c+1]
+    int n_fwd_tiles = 0, n_fwd_ctas = 0;
     int2* d_inv_tiles = nullptr;
-    int n_inv_tiles = 0;
+    int* d_inv_off = nullptr;
+    int n_inv_tiles = 0, n_inv_ctas = 0;
     int m_tc_end = 0;         // orders m < m_tc_end go through the tensor cores
     int Lh = 0;               // rows per (m, parity) of the synthesis operand
     void* encode = nullptr;   // cuTensorMapEncodeTiled (driver entry point)
@@ -274,7 +294,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  float* __restrict__ alm, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
                  const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
                  const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
-                 const int2* __restrict__ tiles, int ntiles, int accumulate, const unsigned* __restrict__ fmax,
+                 const int2* __restrict__ tiles, const int* __restrict__ tile_off, int accumulate,
+                 const unsigned* __restrict__ fmax,
                  float wb, int* __restrict__ err) {
     __shared__ float s_inv[kTcCols / 2];
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -286,6 +307,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = 2 * nside;
     const int nbk = seed_blocks(L);
+    const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, fmax, wb, nmaps);
     tc_setup(sh, kFStages, 1, warp);
     const uint32_t tmem = sh->tmem_base;
@@ -296,7 +318,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc::tma_prefetch_desc(&xh_map);
             tc::tma_prefetch_desc(&xl_map);
             int it = 0;
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            for (int t = t_begin; t < t_end; ++t) {
                 const int m = tiles[t].x;
                 const int t0 = first_ring_for_m(m, nside);
                 const int nch = nchunks(m);
@@ -322,9 +344,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
+            TCP_DECL;
+            TCP_T0(role);
             const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, true, true) : tc::idesc_bf16(128, kTcCols, true, true);
             int it = 0, tcount = 0;
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+            for (int t = t_begin; t < t_end; ++t, ++tcount) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
                 TCP_T0(w2);
@@ -360,12 +384,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         mma_done:
             mma_drain(sh);
+            TCP_ADD(0, 10, role);
+            TCP_FLUSH(0);
         }
     } else if (warp >= 4 && warp < 8) {
         // ------------------------------------------------ epilogue: TMEM -> alm
+        TCP_DECL;
         const int ew = warp & 3;  // TMEM lanes 32*ew .. +31
         int tcount = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+        for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, jb = tiles[t].y;
             const int l0 = m + jb * kTcFwdDeg;
             // zero the l < m triangle of this column while the tile accumulates
@@ -417,15 +444,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane == 0) tc::mbar_arrive(&sh->acc_empty[0]);
             if (lane == 0) TCP_ADD(0, 6, e1);
         }
+        if (lane == 0) TCP_FLUSH(0);
     } else if (warp >= 8 && warp < 8 + kFStages) {
         // ------------------------------------------------ Pbar producers
+        TCP_DECL;
         const int pw = warp - 8;
         const int r = lane & 15, bp = lane >> 4;
         AlphaC* cfw = coef_s + pw * kFCoef;
-        int t = blockIdx.x, c = 0, it = 0, cur_tile = -1;
+        int t = t_begin, c = 0, it = 0, cur_tile = -1;
         int m = 0, jb = 0, t0 = 0, nch = 0;
         auto load_tile = [&]() {
-            if (t < ntiles) {
+            if (t < t_end) {
                 const int2 tt = tiles[t];
                 m = tt.x;
                 jb = tt.y;
@@ -434,9 +463,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         };
         auto to_mine = [&]() {
-            while (t < ntiles) {
+            while (t < t_end) {
                 if (c >= nch) {
-                    t += gridDim.x;
+                    ++t;
                     c = 0;
                     load_tile();
                     continue;
@@ -469,8 +498,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         };
         load_tile();
         to_mine();
-        if (t < ntiles) {
+        if (t < t_end) {
             In cur = fetch();
+            TCP_T0(lp);
             while (true) {
                 const int s = cur.it % kFStages;
                 if (cur.tile != cur_tile) {
@@ -481,6 +511,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     __syncwarp();
                     cur_tile = cur.tile;
                 }
+                if (lane == 0) TCP_ADD(0, 8, lp);
                 TCP_T0(pw0);
                 if (!tc::mbar_wait_warp(&sh->empty[s], ((cur.it / kFStages) & 1) ^ 1, err, 16)) break;
                 if (lane == 0) TCP_ADD(0, 3, pw0);
@@ -500,6 +531,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 };
                 const int b0 = cur.l0 + 128 * bp;
                 const bool fast = cur.l0 >= cur.lsm;  // warp-uniform
+                TCP_T0(gg);
                 if (fast) {
                     gen2_fast(cur.s0, cur.s1, cur.x, cur.x, cfw + 128 * bp, cfw + 128 * bp + 64, emit);
                 } else {
@@ -510,19 +542,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     gen1_slow(0, cur.m, b0, L, Lpad, ls, ps, cur.s0, v ? cur.x : 0.0, coef, emit);
                     gen1_slow(1, cur.m, b0 + 64, L, Lpad, ls, ps, cur.s1, v ? cur.x : 0.0, coef, emit);
                 }
+                if (lane == 0) TCP_ADD(0, 7, gg);
+                TCP_T0(ff);
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sh->full_prod[s]);
+                if (lane == 0) TCP_ADD(0, 9, ff);
                 if (lane == 0) TCP_ADD(0, 4, pw1);
+                TCP_SET(lp);
                 // next chunk's inputs: issued after this chunk is published, so the
                 // proxy fence and the release-arrive above never wait on them
                 ++c;
                 ++it;
                 to_mine();
-                if (t >= ntiles) break;
+                if (t >= t_end) break;
                 cur = fetch();
             }
         }
+        if (lane == 0) TCP_FLUSH(0);
     }
 
     tc::tc_fence_before();
@@ -549,7 +586,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                  const double* __restrict__ zr, const int* __restrict__ lstart, const int* __restrict__ lsmax,
                  const double2* __restrict__ pstart, const double2* __restrict__ coef,
                  const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds, const int2* __restrict__ tiles,
-                 int ntiles, const unsigned* __restrict__ amax, int* __restrict__ err) {
+                 const int* __restrict__ tile_off, const unsigned* __restrict__ amax, int* __restrict__ err) {
     __shared__ float s_inv[kTcCols / 2];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // align by pointer arithmetic on the shared array (keeps the shared address space known)
@@ -560,6 +597,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = 2 * nside;
     const int nbk = seed_blocks(L);
+    const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, amax, 1.f, nmaps);
     tc_setup(sh, kIStages, 2, warp);
     const uint32_t tmem = sh->tmem_base;
@@ -570,7 +608,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc::tma_prefetch_desc(&ah_map);
             tc::tma_prefetch_desc(&al_map);
             int it = 0;
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            for (int t = t_begin; t < t_end; ++t) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
@@ -594,9 +632,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
+            TCP_DECL;
+            TCP_T0(role);
             const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, false, true) : tc::idesc_bf16(128, kTcCols, false, true);
             int it = 0, tcount = 0;
-            for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+            for (int t = t_begin; t < t_end; ++t, ++tcount) {
                 const int m = tiles[t].x;
                 const int nch = nchunks(m);
                 TCP_T0(w2);
@@ -636,17 +676,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         mma_done:
             mma_drain(sh);
+            TCP_ADD(1, 10, role);
+            TCP_FLUSH(1);
         }
     } else if (warp >= 4 && warp < 8) {
         // ------------------------------------------------ epilogue: TMEM -> spec (E, O)
+        TCP_DECL;
         const int ew = warp & 3;
         int tcount = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+        for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, rb = tiles[t].y;
             const int t0 = first_ring_for_m(m, nside);
             const int rr = rb + ew * 32 + lane;
             const int p = t0 + rr;
+            TCP_T0(e0);
             if (!tc::mbar_wait_warp(&sh->acc_full[0], tcount & 1, err, 25)) break;
+            if (lane == 0) TCP_ADD(1, 5, e0);
+            TCP_T0(e1);
             tc::tc_fence_after();
 #pragma unroll 1
             for (int par = 0; par < 2; ++par) {
@@ -671,17 +717,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&sh->acc_empty[0]);
+            if (lane == 0) TCP_ADD(1, 6, e1);
         }
+        if (lane == 0) TCP_FLUSH(1);
     } else if (warp >= 8 && warp < 8 + 2 * kIStages) {
         // ------------------------------------------------ Pbar^T producers
+        TCP_DECL;
         const int pw = warp - 8;
         const int g = pw >> 1, w = pw & 1;
         AlphaC* cfw = coef_s + pw * 64;
         const int r0 = 32 * w + lane, r1 = 64 + 32 * w + lane;  // tile rows of the two chains
-        int t = blockIdx.x, c = 0, it = 0;
+        int t = t_begin, c = 0, it = 0;
         int m = 0, rb = 0, t0 = 0, nch = 0;
         auto load_tile = [&]() {
-            if (t < ntiles) {
+            if (t < t_end) {
                 const int2 tt = tiles[t];
                 m = tt.x;
                 rb = tt.y;
@@ -690,9 +739,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         };
         auto to_mine = [&]() {
-            while (t < ntiles) {
+            while (t < t_end) {
                 if (c >= nch) {
-                    t += gridDim.x;
+                    ++t;
                     c = 0;
                     load_tile();
                     continue;
@@ -728,10 +777,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         };
         load_tile();
         to_mine();
-        if (t < ntiles) {
+        if (t < t_end) {
             In cur = fetch();
+            TCP_T0(lp);
             while (true) {
                 const int s = cur.it % kIStages;
+                if (lane == 0) TCP_ADD(1, 8, lp);
                 TCP_T0(pw0);
                 if (!tc::mbar_wait_warp(&sh->empty[s], ((cur.it / kIStages) & 1) ^ 1, err, 26)) break;
                 if (lane == 0) TCP_ADD(1, 3, pw0);
@@ -752,10 +803,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     st_shared_v4(sa + 2 * 8192 + off, oh);
                     st_shared_v4(sa + 3 * 8192 + off, ol);
                 };
+                TCP_T0(gg);
                 if (cur.l0b >= cur.lsm) {
-                    TCP_T0(gg);
                     gen2_fast(cur.s0, cur.s1, cur.x0, cur.x1, cfw, cfw, emit);
-                    if (lane == 0) TCP_ADD(1, 5, gg);
                 } else {
                     const bool v0 = cur.p0 < NP, v1 = cur.p1 < NP;
                     const int64_t mb = (int64_t)cur.m * NP;
@@ -764,19 +814,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     gen1_slow(1, cur.m, cur.l0b, L, Lpad, v1 ? lstart[mb + cur.p1] : L,
                               v1 ? pstart[mb + cur.p1] : make_double2(0.0, 0.0), cur.s1, cur.x1, coef, emit);
                 }
+                if (lane == 0) TCP_ADD(1, 7, gg);
                 TCP_T0(ff);
                 tc::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&sh->full_prod[s]);
-                if (lane == 0) TCP_ADD(1, 6, ff);
+                if (lane == 0) TCP_ADD(1, 9, ff);
                 if (lane == 0) TCP_ADD(1, 4, pw1);
+                TCP_SET(lp);
                 ++c;
                 ++it;
                 to_mine();
-                if (t >= ntiles) break;
+                if (t >= t_end) break;
                 cur = fetch();
             }
         }
+        if (lane == 0) TCP_FLUSH(1);
     }
 
     tc::tc_fence_before();
