@@ -427,9 +427,7 @@ def algorithmic(nside, L, M):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per full launch of the
 # dominant kernel, from one single-pass ncu capture of this script's default
 # workload: (stage, nside, lmax, precision) -> bytes
-MEASURED_TRAFFIC = {
-    ("legendre_forward", 1024, 2047, "f16x3"): 14.94e9 + 6.84e9,
-}
+MEASURED_TRAFFIC = {}
 
 
 def roofline(stats, args, prec, refine, nside, L, B):

@@ -22,6 +22,8 @@ STATUS = {
     6: "workspace too small",
 }
 
+FLAG_OTF_LEGENDRE = 1
+
 PRECISIONS = {"fp32": 0, "fp64": 1, "bf16x3": 2, "tf32": 3, "f16x3": 4}
 
 # exported symbols and their signatures (argtypes, restype)
@@ -61,6 +63,7 @@ SIGNATURES = {
     "hpx_sht_inverse_adjoint": ([_vp, _vp, _vp, _i64, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_refined": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_noalloc": ([_vp, _vp, _vp, _i64, _vp], ctypes.c_int),
+    "hpx_plan_table_bytes": ([_vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hpx_plan_info": (
         [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
         ctypes.c_int,

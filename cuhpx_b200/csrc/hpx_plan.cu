@@ -153,6 +153,7 @@ struct hpx_plan_s {
         cudaFree(tc.d_inv_tiles);
         cudaFree(tc.d_fwd_off);
         cudaFree(tc.d_inv_off);
+        cudaFree(tc.d_table);
         for (auto& r : stats_recs) {
             cudaEventDestroy(r.a);
             cudaEventDestroy(r.b);
@@ -173,6 +174,11 @@ struct hpx_plan_s {
     size_t tcA_bytes() const { return mixed() ? (size_t)2 * 2 * M * tc.Lh * kTcCols * sizeof(uint16_t) : 0; }
     // per-map max |F| and max |a| (FP16 operand scales)
     size_t scale_bytes() const { return f16() ? (size_t)2 * 4 * batch_chunk : 0; }
+    // order-major analysis output of the tensor cores, ycols[m][l][128]; it
+    // reuses the ring-spectra region (dead after the fold) when that is large
+    // enough, else the SIMT column region
+    size_t ycols_bytes() const { return mixed() ? (size_t)tc.m_tc_end * L * kTcCols * sizeof(float) : 0; }
+    bool ycols_in_F() const { return F_bytes() >= ycols_bytes(); }
 };
 
 namespace {
@@ -267,6 +273,53 @@ int schedule_tiles(const std::vector<int2>& tiles, const std::vector<double>& co
     return nc;
 }
 
+// Tensor map over the resident table [4 m_tc_end][2N][Lt] of 2-byte halves.
+int encode_table(const hpx_plan_s* P, CUtensorMap* map, int box_i, int box_rings, CUtensorMapSwizzle sw) {
+    const TcPlan& T = P->tc;
+    const cuuint64_t dims[3] = {(cuuint64_t)T.Lt, (cuuint64_t)P->NP, (cuuint64_t)4 * T.m_tc_end};
+    const cuuint64_t strides[2] = {(cuuint64_t)T.Lt * 2, (cuuint64_t)T.Lt * 2 * P->NP};
+    const cuuint32_t box[3] = {(cuuint32_t)box_i, (cuuint32_t)box_rings, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = ((EncodeTiledFn)T.encode)(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, T.d_table, dims, strides, box, es,
+                                           CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(HPX_ERR_CUDA, "cuTensorMapEncodeTiled (table) failed: " + std::to_string((int)r));
+    return HPX_OK;
+}
+
+// Resident Legendre table (see HPX_FLAG_OTF_LEGENDRE): kept when it fits in
+// 45% of the device memory and leaves 4 GB free; otherwise the producer warps
+// generate Pbar on the fly.
+int tc_table_create(hpx_plan_s* P) {
+    TcPlan& T = P->tc;
+    T.table = 0;
+    if ((P->desc.flags & HPX_FLAG_OTF_LEGENDRE) || T.m_tc_end == 0) return HPX_OK;
+    T.Lt = ((P->L + 1) / 2 + 7) & ~7;
+    const size_t bytes = (size_t)4 * T.m_tc_end * P->NP * T.Lt * sizeof(uint16_t);
+    size_t free_b = 0, total_b = 0;
+    HPX_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if ((double)bytes > 0.45 * (double)total_b || bytes + ((size_t)4 << 30) > free_b) return HPX_OK;
+    HPX_CUDA_TRY(cudaMalloc(&T.d_table, bytes));
+    HPX_CUDA_TRY(cudaMemset(T.d_table, 0, bytes));
+    const int64_t n = (int64_t)T.m_tc_end * seed_blocks(P->L) * P->NP;
+    const unsigned grid = (unsigned)((n + 127) / 128);
+    if (P->f16())
+        k_legendre_table<true><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->nside, T.Lt, P->d_z, P->d_lstart,
+                                              P->d_pstart, P->d_coef, P->d_seeds, T.d_table);
+    else
+        k_legendre_table<false><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->nside, T.Lt, P->d_z, P->d_lstart,
+                                               P->d_pstart, P->d_coef, P->d_seeds, T.d_table);
+    HPX_CUDA_TRY(cudaGetLastError());
+    HPX_CUDA_TRY(cudaDeviceSynchronize());
+    int rc = encode_table(P, &T.tab_fwd, 64, kFRing, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc != HPX_OK) return rc;
+    rc = encode_table(P, &T.tab_inv, kTcDegChunk / 2, kTcInvRings, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (rc != HPX_OK) return rc;
+    T.table_bytes = bytes;
+    T.table = 1;
+    return HPX_OK;
+}
+
 // Tensor-core plan: tile lists, error flag, tensor-map encoder.
 int tc_create(hpx_plan_s* P) {
     TcPlan& T = P->tc;
@@ -283,6 +336,8 @@ int tc_create(hpx_plan_s* P) {
     const int N = P->nside;
     T.m_tc_end = std::min(std::min(P->L, P->M), 2 * N + 1);
     T.Lh = (P->L + 65) / 2;
+    const int rc = tc_table_create(P);
+    if (rc != HPX_OK) return rc;
     std::vector<int2> ft, it;
     for (int m = 0; m < T.m_tc_end; ++m) {
         for (int j = 0; j < (P->L - m + kTcFwdDeg - 1) / kTcFwdDeg; ++j) ft.push_back(make_int2(m, j));
@@ -291,11 +346,13 @@ int tc_create(hpx_plan_s* P) {
     }
     T.n_fwd_tiles = (int)ft.size();
     T.n_inv_tiles = (int)it.size();
-    // Tile costs in producer chunks: a chunk whose degrees start below the
-    // order's largest first significant degree takes the slower
-    // start-injecting recurrence (about twice the time); every tile also pays
-    // a fixed epilogue of about seven chunks.
-    constexpr double kSlow = 2.0, kTileFixed = 7.0;
+    // Tile costs in pipeline chunks, plus a fixed epilogue of about seven
+    // chunks per tile.  Without the resident table, a chunk whose degrees
+    // start below the order's largest first significant degree takes the
+    // producers' slower start-injecting recurrence (about twice the time);
+    // with it every chunk costs the same, and the tiles of one order sort
+    // together, run at the same time and share its data operand in L2.
+    const double kSlow = T.table ? 1.0 : 2.0, kTileFixed = 7.0;
     std::vector<double> fc, ic;
     for (const int2& t : ft) {
         const int nch = (P->NP - first_ring_for_m(t.x, N) + kFRing - 1) / kFRing;
@@ -322,10 +379,14 @@ int tc_create(hpx_plan_s* P) {
         HPX_CUDA_TRY(cudaMalloc(&T.d_inv_off, sizeof(int) * off.size()));
         HPX_CUDA_TRY(cudaMemcpy(T.d_inv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
     }
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_tc<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kISmem));
     T.active = 1;
     return HPX_OK;
 }
@@ -545,6 +606,7 @@ struct Pipeline {
     T* almT;
     T* resid;
     uint16_t* tcA;  // bf16/fp16 hi/lo synthesis operand (mixed plans)
+    float* ycols_alt = nullptr;  // ycols region when the ring spectra region is too small
     unsigned* fmax = nullptr;  // per-map max |F| (FP16 plans)
     unsigned* amax = nullptr;  // per-map max |a| (FP16 plans)
     float fold_wb = 0.f;       // bound on the fold factor |c| (F_t + F_t') / max|F|
@@ -563,6 +625,7 @@ struct Pipeline {
         F = (T*)c;
         c += (P->F_bytes() + 255) & ~(size_t)255;
         set_scales(c);
+        ycols_alt = (float*)almT;
     }
     void set_scales(char* c) {
         if (!P->f16()) return;
@@ -570,9 +633,10 @@ struct Pipeline {
         amax = fmax + P->batch_chunk;
     }
     // analysis-only layout: folded spectra and ring spectra at given addresses
-    Pipeline(const hpx_plan_s* p, T* spec_, T* F_, char* scales, cudaStream_t s)
+    Pipeline(const hpx_plan_s* p, T* spec_, T* F_, char* scales, float* ycols, cudaStream_t s)
         : P(p), st(s), spec(spec_), almT(nullptr), resid(nullptr), tcA(nullptr), F(F_) {
         set_scales(scales);
+        ycols_alt = ycols;
     }
     T* F;  // ring-major spectra [map][Ftot] complex
     // folded spectra as bf16 hi/lo (mixed plans), aliasing the spec region
@@ -648,11 +712,15 @@ struct Pipeline {
             CUtensorMap mh, ml;
             if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
-            auto kern = P->f16() ? k_leg_fwd_tc<true> : k_leg_fwd_tc<false>;
+            float* yc = (float*)(P->ycols_in_F() ? (void*)F : (void*)ycols_alt);
+            auto kern = TP.table ? (P->f16() ? k_leg_fwd_tc<true, true> : k_leg_fwd_tc<false, true>)
+                                 : (P->f16() ? k_leg_fwd_tc<true, false> : k_leg_fwd_tc<false, false>);
             kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(
-                mh, ml, nb, (float*)alm, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
-                P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, accumulate, fmax,
+                mh, ml, TP.table ? TP.tab_fwd : mh, nb, yc, P->L, P->Lpad, P->nside, P->d_z, P->d_lstart,
+                P->d_lsmax, P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, fmax,
                 fold_wb, TP.d_err);
+            dim3 tg((TP.m_tc_end + 31) / 32, P->L);
+            k_tc_to_alm<<<tg, dim3(32, 8), 0, st>>>(yc, nb, P->L, P->M, TP.m_tc_end, (float*)alm, accumulate);
             return;
         }
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
@@ -686,9 +754,10 @@ struct Pipeline {
             CUtensorMap mh, ml;
             if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
-            auto kern = P->f16() ? k_leg_inv_tc<true> : k_leg_inv_tc<false>;
+            auto kern = TP.table ? (P->f16() ? k_leg_inv_tc<true, true> : k_leg_inv_tc<false, true>)
+                                 : (P->f16() ? k_leg_inv_tc<true, false> : k_leg_inv_tc<false, false>);
             kern<<<TP.n_inv_ctas, kTcThreads, kISmem, st>>>(
-                mh, ml, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
+                mh, ml, TP.table ? TP.tab_inv : mh, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
                 P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.d_inv_off, amax, TP.d_err);
             return;
         }
@@ -779,7 +848,12 @@ size_t noalloc_spec_offset(const hpx_plan_s* P) { return (P->spec_bytes() + 255)
 size_t noalloc_scale_offset(const hpx_plan_s* P) {
     return noalloc_spec_offset(P) + ((P->F_bytes() + 255) & ~(size_t)255);
 }
-size_t noalloc_need(const hpx_plan_s* P) { return noalloc_scale_offset(P) + P->scale_bytes(); }
+size_t noalloc_ycols_offset(const hpx_plan_s* P) {
+    return noalloc_scale_offset(P) + ((P->scale_bytes() + 255) & ~(size_t)255);
+}
+size_t noalloc_need(const hpx_plan_s* P) {
+    return noalloc_ycols_offset(P) + (P->ycols_in_F() ? 0 : P->ycols_bytes());
+}
 
 }  // namespace
 
@@ -816,7 +890,8 @@ int noalloc_scratch(int device, unsigned char** out) {
 template <typename T>
 int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch, unsigned char* scratch,
                         cudaStream_t st) {
-    Pipeline<T> pl(P, (T*)scratch, (T*)(scratch + noalloc_spec_offset(P)), (char*)scratch + noalloc_scale_offset(P), st);
+    Pipeline<T> pl(P, (T*)scratch, (T*)(scratch + noalloc_spec_offset(P)), (char*)scratch + noalloc_scale_offset(P),
+                   (float*)(scratch + noalloc_ycols_offset(P)), st);
     const int64_t bc = P->batch_chunk;
     const size_t alm_stride = (size_t)P->L * P->M * 2;
     for (int64_t b0 = 0; b0 < batch; b0 += bc) {
@@ -869,7 +944,7 @@ int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan) {
         return set_err(HPX_ERR_INVALID_ARG, "unknown precision");
     if (desc->batch_chunk < 0 || desc->batch_chunk > 4096) return set_err(HPX_ERR_INVALID_ARG, "batch_chunk out of range");
     if (desc->refine_iters < 0 || desc->refine_iters > 64) return set_err(HPX_ERR_INVALID_ARG, "refine_iters out of range");
-    if (desc->flags != 0) return set_err(HPX_ERR_INVALID_ARG, "flags must be 0");
+    if (desc->flags & ~HPX_FLAG_OTF_LEGENDRE) return set_err(HPX_ERR_INVALID_ARG, "unknown flag bits");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -935,6 +1010,12 @@ int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_gra
 int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, void* ws,
                             size_t ws_bytes, void* stream) {
     return dispatch(plan, kInverseAdjoint, map_grad, alm_grad, batch, ws, ws_bytes, stream);
+}
+
+int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes) {
+    if (!plan || !bytes) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    *bytes = plan->tc.table ? plan->tc.table_bytes : 0;
+    return HPX_OK;
 }
 
 int hpx_plan_check(hpx_plan_t plan, void* stream) {

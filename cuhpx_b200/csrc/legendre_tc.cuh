@@ -101,6 +101,11 @@ struct TcPlan {
     int* d_inv_off = nullptr;
     int n_inv_tiles = 0, n_inv_ctas = 0;
     int m_tc_end = 0;         // orders m < m_tc_end go through the tensor cores
+    int table = 0;            // 1: Pbar read from the resident table, 0: generated by producer warps
+    int Lt = 0;               // table row length (halves)
+    size_t table_bytes = 0;
+    uint16_t* d_table = nullptr;  // [m_tc_end][2 par][2 hl][2N][Lt]
+    CUtensorMap tab_fwd{}, tab_inv{};
     int Lh = 0;               // rows per (m, parity) of the synthesis operand
     void* encode = nullptr;   // cuTensorMapEncodeTiled (driver entry point)
 };
@@ -278,6 +283,87 @@ __device__ __forceinline__ void gen1_slow(int chain, int m, int l0b, int L, int 
     }
 }
 
+// ================================================================== resident table
+// Legendre table of the tensor-core contraction: tab[m][par][hl][p][i] (2-byte
+// halves; row length Lt, a multiple of 8) holds Pbar_l^m(z_p) for l = m + 2i +
+// par, rounded from FP64 to FP32 and split into hi + lo halves (fp16 or bf16).
+// The rows are l-contiguous, so TMA boxes of {64 i, 16 rings} (128B swizzle)
+// and {32 i, 128 rings} (64B swizzle) land exactly in the analysis and
+// synthesis A-operand layouts.  Thread per (m, north ring p >= first ring of
+// m, 64-degree block), starting from the block seed (or, inside the block
+// holding the first significant degree, from the start pair), as gen1_slow.
+// Entries never written (rings before the first ring of m, degrees >= L)
+// must be zero: the caller clears the table first.
+template <bool F16>
+__global__ void __launch_bounds__(128) k_legendre_table(int m_end, int L, int Lpad, int nside, int Lt,
+                                                        const double* __restrict__ zr, const int* __restrict__ lstart,
+                                                        const double2* __restrict__ pstart,
+                                                        const double2* __restrict__ coef,
+                                                        const double2* __restrict__ seeds, uint16_t* __restrict__ tab) {
+    const int NP = 2 * nside;
+    const int nbk = seed_blocks(L);
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)m_end * nbk * NP) return;
+    const int p = (int)(idx % NP);
+    const int j = (int)((idx / NP) % nbk);
+    const int m = (int)(idx / ((int64_t)NP * nbk));
+    const int l0 = m + j * kSeedBlock;
+    if (l0 >= L || p < first_ring_for_m(m, nside)) return;
+    const int64_t mi = (int64_t)m * NP + p;
+    const int ls = lstart[mi];
+    const double2 ps = pstart[mi];
+    const double2 sd = seeds[((int64_t)m * nbk + j) * NP + p];
+    const double x = zr[p];
+    double p1 = 0.0, p2 = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {  // 16 degrees -> 8 values of each parity
+        uint32_t hi[2][4], lo[2][4];
+#pragma unroll
+        for (int k = 0; k < 16; k += 2) {
+            float f[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int kk = q * 16 + k + u, l = l0 + kk;
+                double v;
+                if (kk == 0 && ls <= l0) v = sd.x;
+                else if (kk == 1 && ls <= l0) v = sd.y;
+                else {
+                    const double2 ab = (l < L && l >= m + 2) ? coef[(int64_t)m * Lpad + l] : make_double2(0.0, 0.0);
+                    v = (l < L) ? leg_step(l, ls, ps, ab.x, ab.y, x, p1, p2) : 0.0;
+                }
+                p2 = p1;
+                p1 = v;
+                f[u] = (float)v;
+            }
+            // f[0]: even offset (par 0), f[1]: odd offset (par 1), index i = 8q + k/2
+            const int w = (k >> 1) >> 1, half = (k >> 1) & 1;
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+                uint16_t h, g;
+                if (F16) tc::split_f16(f[par], h, g);
+                else tc::split_bf16(f[par], h, g);
+                if (half == 0) {
+                    hi[par][w] = h;
+                    lo[par][w] = g;
+                } else {
+                    hi[par][w] |= (uint32_t)h << 16;
+                    lo[par][w] |= (uint32_t)g << 16;
+                }
+            }
+        }
+        const int i0 = j * (kSeedBlock / 2) + q * 8;
+        if (i0 < Lt) {
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+                uint16_t* rh = tab + ((((int64_t)m * 2 + par) * 2 + 0) * NP + p) * Lt + i0;
+                uint16_t* rl = tab + ((((int64_t)m * 2 + par) * 2 + 1) * NP + p) * Lt + i0;
+                *(uint4*)rh = make_uint4(hi[par][0], hi[par][1], hi[par][2], hi[par][3]);
+                *(uint4*)rl = make_uint4(lo[par][0], lo[par][1], lo[par][2], lo[par][3]);
+            }
+        }
+    }
+}
+
 // ================================================================== analysis
 // Xh/Xl: bf16 [2M][NP][128] (hi and lo of S (par 0) and D (par 1)) via tensor maps.
 // Tile (m, 256 degrees); pipeline chunk = 16 rings.  Stage layout:
@@ -288,14 +374,14 @@ __device__ __forceinline__ void gen1_slow(int chain, int m, int l0b, int L, int 
 // producer groups than stages an mbarrier parity wait could pass on a stale
 // phase).  Lane = (ring r = lane&15, block pair bp = lane>>4) runs the two
 // blocks 2bp, 2bp+1 of its ring.
-template <bool F16>
+template <bool F16, bool TAB>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map, int nmaps,
-                 float* __restrict__ alm, int L, int M, int Lpad, int nside, const double* __restrict__ zr,
+    k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map,
+                 const __grid_constant__ CUtensorMap tab_map, int nmaps,
+                 float* __restrict__ ycols, int L, int Lpad, int nside, const double* __restrict__ zr,
                  const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
                  const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
-                 const int2* __restrict__ tiles, const int* __restrict__ tile_off, int accumulate,
-                 const unsigned* __restrict__ fmax,
+                 const int2* __restrict__ tiles, const int* __restrict__ tile_off, const unsigned* __restrict__ fmax,
                  float wb, int* __restrict__ err) {
     __shared__ float s_inv[kTcCols / 2];
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -317,17 +403,27 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (lane == 0) {
             tc::tma_prefetch_desc(&xh_map);
             tc::tma_prefetch_desc(&xl_map);
+            if (TAB) tc::tma_prefetch_desc(&tab_map);
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
-                const int m = tiles[t].x;
+                const int m = tiles[t].x, jb = tiles[t].y;
                 const int t0 = first_ring_for_m(m, nside);
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kFStages;
                     if (!tc::mbar_wait(&sh->empty[s], ((it / kFStages) & 1) ^ 1, err, 11)) goto tma_done;
                     unsigned char* st = stages + s * kFStageBytes + 16384;
-                    tc::mbar_arrive_tx(&sh->full_tma[s], 16384);
+                    tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? 32768 : 16384);
                     const int y = t0 + c * kFRing;
+                    if (TAB) {
+                        // A operand: Pbar for 128 degrees of each parity x 16 rings, hi and lo
+#pragma unroll
+                        for (int ph = 0; ph < 4; ++ph)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+                                tc::tma_load_3d(stages + s * kFStageBytes + ph * 4096 + h * 2048, &tab_map,
+                                                jb * (kTcFwdDeg / 2) + h * 64, y, 4 * m + ph, &sh->full_tma[s]);
+                    }
 #pragma unroll
                     for (int par = 0; par < 2; ++par)
 #pragma unroll
@@ -362,7 +458,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!tc::mbar_wait(&sh->full_tma[s], ph, err, 13)) goto mma_done;
                     TCP_ADD(0, 0, w0);
                     TCP_T0(w1);
-                    if (!tc::mbar_wait(&sh->full_prod[s], ph, err, 14)) goto mma_done;
+                    if (!TAB && !tc::mbar_wait(&sh->full_prod[s], ph, err, 14)) goto mma_done;
                     TCP_ADD(0, 1, w1);
                     tc::tc_fence_after();
                     const uint32_t sa = tc::smem_u32(stages + s * kFStageBytes);
@@ -388,21 +484,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             TCP_FLUSH(0);
         }
     } else if (warp >= 4 && warp < 8) {
-        // ------------------------------------------------ epilogue: TMEM -> alm
+        // ------------------------------------------------ epilogue: TMEM -> ycols[m][l][128]
+        // Each row (m, l) is written whole by one thread (512 contiguous bytes),
+        // so no two CTAs write the same sector; k_tc_to_alm scatters the rows
+        // into alm[b][l][m] with coalesced stores.
         TCP_DECL;
         const int ew = warp & 3;  // TMEM lanes 32*ew .. +31
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, jb = tiles[t].y;
             const int l0 = m + jb * kTcFwdDeg;
-            // zero the l < m triangle of this column while the tile accumulates
-            if (!accumulate && jb == 0) {
-                const int nz = min(m, L);
-                for (int i = (warp - 4) * 32 + lane; i < nz * 64; i += 128) {
-                    const int l = i >> 6, b = i & 63;
-                    if (b < nmaps) *(float2*)(alm + 2 * (((int64_t)b * L + l) * M + m)) = make_float2(0.f, 0.f);
-                }
-            }
             TCP_T0(e0);
             if (!tc::mbar_wait_warp(&sh->acc_full[0], tcount & 1, err, 15)) break;
             if (lane == 0) TCP_ADD(0, 5, e0);
@@ -421,20 +512,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] += w[j];
                     if (l < L) {
+                        float* dst = ycols + ((int64_t)m * L + l) * kTcCols + c;
 #pragma unroll
-                        for (int j = 0; j < 16; j += 2) {
-                            const int b = (c + j) >> 1;
-                            if (b < nmaps) {
-                                float2* dst = (float2*)(alm + 2 * (((int64_t)b * L + l) * M + m));
-                                const float sb = s_inv[b];
-                                float2 o = make_float2(v[j] * sb, v[j + 1] * sb);
-                                if (accumulate) {
-                                    const float2 q = *dst;
-                                    o.x += q.x;
-                                    o.y += q.y;
-                                }
-                                *dst = o;
-                            }
+                        for (int j = 0; j < 16; j += 4) {
+                            const float s0 = s_inv[(c + j) >> 1], s1 = s_inv[((c + j) >> 1) + 1];
+                            *(float4*)(dst + j) = make_float4(v[j] * s0, v[j + 1] * s0, v[j + 2] * s1, v[j + 3] * s1);
                         }
                     }
                 }
@@ -445,7 +527,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane == 0) TCP_ADD(0, 6, e1);
         }
         if (lane == 0) TCP_FLUSH(0);
-    } else if (warp >= 8 && warp < 8 + kFStages) {
+    } else if (!TAB && warp >= 8 && warp < 8 + kFStages) {
         // ------------------------------------------------ Pbar producers
         TCP_DECL;
         const int pw = warp - 8;
@@ -579,9 +661,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // Chunk it goes to producer pair g = it mod 3 (warps 8+2g, 9+2g), which owns
 // stage g (one barrier phase of run-ahead at most); lane runs rings 32w + lane
 // and 64 + 32w + lane of the tile.
-template <bool F16>
+template <bool F16, bool TAB>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_inv_tc(const __grid_constant__ CUtensorMap ah_map, const __grid_constant__ CUtensorMap al_map,
+                 const __grid_constant__ CUtensorMap tab_map,
                  float* __restrict__ spec, int C, int nmaps, int L, int M, int Lpad, int nside,
                  const double* __restrict__ zr, const int* __restrict__ lstart, const int* __restrict__ lsmax,
                  const double2* __restrict__ pstart, const double2* __restrict__ coef,
@@ -607,15 +690,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (lane == 0) {
             tc::tma_prefetch_desc(&ah_map);
             tc::tma_prefetch_desc(&al_map);
+            if (TAB) tc::tma_prefetch_desc(&tab_map);
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
-                const int m = tiles[t].x;
+                const int m = tiles[t].x, rb = tiles[t].y;
+                const int t0 = first_ring_for_m(m, nside);
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kIStages;
                     if (!tc::mbar_wait(&sh->empty[s], ((it / kIStages) & 1) ^ 1, err, 21)) goto tma_done;
                     unsigned char* st = stages + s * kIStageBytes + 32768;
-                    tc::mbar_arrive_tx(&sh->full_tma[s], 32768);
+                    tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? 65536 : 32768);
+                    if (TAB) {
+                        // A operand: Pbar^T for 128 rings x 32 degrees of each parity, hi and lo
+#pragma unroll
+                        for (int ph = 0; ph < 4; ++ph)
+                            tc::tma_load_3d(stages + s * kIStageBytes + ph * 8192, &tab_map, c * (kTcDegChunk / 2),
+                                            t0 + rb, 4 * m + ph, &sh->full_tma[s]);
+                    }
 #pragma unroll
                     for (int par = 0; par < 2; ++par)
 #pragma unroll
@@ -650,7 +742,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!tc::mbar_wait(&sh->full_tma[s], ph, err, 23)) goto mma_done;
                     TCP_ADD(1, 0, w0);
                     TCP_T0(w1);
-                    if (!tc::mbar_wait(&sh->full_prod[s], ph, err, 24)) goto mma_done;
+                    if (!TAB && !tc::mbar_wait(&sh->full_prod[s], ph, err, 24)) goto mma_done;
                     TCP_ADD(1, 1, w1);
                     tc::tc_fence_after();
                     const uint32_t sa = tc::smem_u32(stages + s * kIStageBytes);
@@ -720,7 +812,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane == 0) TCP_ADD(1, 6, e1);
         }
         if (lane == 0) TCP_FLUSH(1);
-    } else if (warp >= 8 && warp < 8 + 2 * kIStages) {
+    } else if (!TAB && warp >= 8 && warp < 8 + 2 * kIStages) {
         // ------------------------------------------------ Pbar^T producers
         TCP_DECL;
         const int pw = warp - 8;
@@ -879,6 +971,37 @@ __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int
             rh[b] = pack_bf16x2(h0, h1);
             rl[b] = pack_bf16x2(l0, l1);
         }
+    }
+}
+
+// ycols[m][l][2b + {re, im}] (analysis output of the tensor cores, orders
+// m < m_end) -> alm[b][l][m] (FP32 complex), storing or (accumulate) adding;
+// l < m entries are set to zero unless accumulating.  Grid (ceil(m_end/32), L),
+// block 32 x 8; the transpose goes through shared memory so that both the
+// 512-byte row reads and the 32-order stores are coalesced.
+__global__ void k_tc_to_alm(const float* __restrict__ ycols, int nmaps, int L, int M, int m_end,
+                            float* __restrict__ alm, int accumulate) {
+    __shared__ float2 tile[64][33];
+    const int m0 = blockIdx.x * 32, l = blockIdx.y;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int mi = ty; mi < 32; mi += 8) {
+        const int m = m0 + mi;
+        const bool live = m < m_end && m <= l;
+        const float2* row = (const float2*)(ycols + ((int64_t)m * L + l) * kTcCols);
+        for (int b = tx; b < 64; b += 32) tile[b][mi] = live ? row[b] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int m = m0 + tx;
+    if (m >= m_end) return;
+    for (int b = ty; b < nmaps && b < 64; b += 8) {
+        float2* dst = (float2*)(alm + 2 * (((int64_t)b * L + l) * M + m));
+        float2 v = tile[b][tx];
+        if (accumulate) {
+            const float2 q = *dst;
+            v.x += q.x;
+            v.y += q.y;
+        }
+        *dst = v;
     }
 }
 

@@ -22,7 +22,9 @@ Differences from the reference, all deliberate:
 * keyword-only extras: ``precision`` ('fp32'; 'f16x3' or 'bf16x3': tcgen05
   tensor cores with a three-term fp16 (per-map power-of-two scaled, ~22-bit)
   or bf16 (~16-bit) split and FP32 accumulation),
-  ``refine_iters`` (Jacobi refinement of the analysis), ``batch_chunk``.
+  ``refine_iters`` (Jacobi refinement of the analysis), ``batch_chunk``,
+  ``legendre_table`` (tensor-core plans: keep the Legendre values resident on
+  the device when they fit, default; False generates them on the fly).
 """
 
 import ctypes
@@ -42,7 +44,8 @@ _plans = {}
 class Plan:
     """One ``hpx_plan_t``: immutable, shareable between modules and streams."""
 
-    def __init__(self, nside, lmax, mmax, quad_weights="ring", precision="fp32", device=0, batch_chunk=64, refine_iters=0):
+    def __init__(self, nside, lmax, mmax, quad_weights="ring", precision="fp32", device=0, batch_chunk=64, refine_iters=0,
+                 legendre_table=True):
         lib = _lib.load()
         if precision not in _lib.PRECISIONS:
             raise ValueError(f"unknown precision {precision!r}; expected one of {sorted(_lib.PRECISIONS)}")
@@ -60,7 +63,7 @@ class Plan:
         desc.refine_iters = int(refine_iters)
         desc.batch_chunk = int(batch_chunk)
         desc.device = self.device
-        desc.flags = 0
+        desc.flags = 0 if legendre_table else _lib.FLAG_OTF_LEGENDRE
         self._w = None
         if quad_weights == "ring":
             self._w = np.ascontiguousarray(read_ring_weight(self.nside), dtype=np.float64)
@@ -84,6 +87,13 @@ class Plan:
         dev = torch.device("cuda", self.device) if device is None else device
         stream = torch.cuda.current_stream(dev).cuda_stream
         _lib.check(self._lib.hpx_plan_check(self._h, ctypes.c_void_p(stream)), self._h)
+
+    @property
+    def table_bytes(self):
+        """Bytes of the resident Legendre table (0: values generated on the fly)."""
+        n = ctypes.c_size_t()
+        _lib.check(self._lib.hpx_plan_table_bytes(self._h, ctypes.byref(n)), self._h)
+        return n.value
 
     # ------------------------------------------------------------------ stats
     def stats_enable(self, on=True):
@@ -159,12 +169,13 @@ class Plan:
         return out
 
 
-def get_plan(nside, lmax, mmax, quad_weights, precision, device, batch_chunk=64):
-    key = (int(nside), int(lmax), int(mmax), quad_weights if quad_weights == "ring" else "none", precision, int(device), int(batch_chunk))
+def get_plan(nside, lmax, mmax, quad_weights, precision, device, batch_chunk=64, legendre_table=True):
+    key = (int(nside), int(lmax), int(mmax), quad_weights if quad_weights == "ring" else "none", precision, int(device),
+           int(batch_chunk), bool(legendre_table))
     with _plan_lock:
         p = _plans.get(key)
         if p is None:
-            p = Plan(nside, lmax, mmax, key[3], precision, device, batch_chunk)
+            p = Plan(nside, lmax, mmax, key[3], precision, device, batch_chunk, legendre_table=key[7])
             _plans[key] = p
         return p
 
@@ -219,7 +230,8 @@ def _device_index(x):
 
 
 class _Base(nn.Module):
-    def __init__(self, nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk):
+    def __init__(self, nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
+                 legendre_table=True):
         super().__init__()
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA device is not available. This class requires a GPU.")
@@ -236,17 +248,20 @@ class _Base(nn.Module):
         self.precision = precision
         self.refine_iters = int(refine_iters)
         self.batch_chunk = int(batch_chunk)
+        self.legendre_table = bool(legendre_table)
         _lib.load()  # fail loudly at construction if the library is missing
 
     def _plan(self, dtype, device_index):
         prec = "fp64" if dtype == torch.float64 else self.precision
-        return get_plan(self.nside, self.lmax, self.mmax, self.quad_weights, prec, device_index, self.batch_chunk)
+        return get_plan(self.nside, self.lmax, self.mmax, self.quad_weights, prec, device_index, self.batch_chunk,
+                        self.legendre_table)
 
 
 class SHTCUDA(_Base):
     def __init__(self, nside, lmax=None, mmax=None, quad_weights="ring", norm="ortho", csphase=True, *,
-                 precision="fp32", refine_iters=0, batch_chunk=64):
-        super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk)
+                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True):
+        super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
+                         legendre_table)
 
     def forward(self, x):
         if torch.is_complex(x):
@@ -264,8 +279,9 @@ class SHTCUDA(_Base):
 
 class iSHTCUDA(_Base):
     def __init__(self, nside, lmax=None, mmax=None, quad_weights="ring", norm="ortho", csphase=True, *,
-                 precision="fp32", refine_iters=0, batch_chunk=64):
-        super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk)
+                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True):
+        super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
+                         legendre_table)
 
     def forward(self, x):
         if not x.is_cuda:

@@ -72,11 +72,19 @@ typedef struct {
     int32_t refine_iters;        /* default Jacobi iterations of hpx_sht_forward_refined */
     int32_t batch_chunk;         /* maps per internal pass (0 = default 64)           */
     int32_t device;              /* CUDA device ordinal the plan lives on             */
-    int32_t flags;               /* reserved, must be 0                               */
+    int32_t flags;               /* HPX_FLAG_* bits, 0 by default                     */
     const double* ring_weights;  /* host array of 2*nside FITS ring-weight corrections
                                     (1 + w) factors are applied inside; NULL = uniform
                                     4*pi/npix ("none" quadrature)                     */
 } hpx_desc_t;
+
+/* Tensor-core plans (F16X3, BF16X3) keep the normalised Legendre values of
+ * every (m, l, ring) resident on the device as hi/lo halves, 8 bytes per
+ * (m, ring, degree pair) (34 GB at nside 1024, lmax = mmax = 2047), when that
+ * fits in 45% of the device memory; the contraction then streams them with
+ * TMA.  With this flag, or when the table does not fit, producer warps
+ * generate them on the fly from FP64 seeds instead (slower, no table). */
+#define HPX_FLAG_OTF_LEGENDRE 1
 
 typedef struct hpx_plan_s* hpx_plan_t;
 
@@ -144,6 +152,9 @@ HPX_API int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stage
 /* Synchronise `stream` and report whether a kernel of this plan gave up on a
  * bounded pipeline wait since the last check (HPX_ERR_TIMEOUT, flag cleared). */
 HPX_API int hpx_plan_check(hpx_plan_t plan, void* stream);
+
+/* Bytes of the plan's resident Legendre table (0 when it has none). */
+HPX_API int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes);
 
 /* Plan geometry queries. */
 HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);

@@ -70,7 +70,7 @@ def _desc(**kw):
 
 @pytest.mark.parametrize(
     "kw",
-    [dict(nside=0), dict(lmax=0), dict(mmax=-1), dict(precision=9), dict(flags=1), dict(batch_chunk=-2), dict(refine_iters=-1)],
+    [dict(nside=0), dict(lmax=0), dict(mmax=-1), dict(precision=9), dict(flags=4), dict(batch_chunk=-2), dict(refine_iters=-1)],
 )
 def test_plan_create_rejects_bad_descriptors(lib, kw):
     h = ctypes.c_void_p()

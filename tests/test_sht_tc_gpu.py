@@ -46,15 +46,18 @@ TC_CASES = [(4, 9, 9), (8, 17, 17), (8, 31, 17), (8, 9, 17), (8, 17, 5), (16, 33
             (128, 255, 255), (64, 257, 129)]
 
 
+@pytest.mark.parametrize("tab", [True, False], ids=["table", "otf"])
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("nside,L,M", TC_CASES)
-def test_tc_forward(hpx, cuda, nside, L, M, prec):
+def test_tc_forward(hpx, cuda, nside, L, M, prec, tab):
     rng = np.random.default_rng(nside + L + M)
     f = rng.standard_normal((3, 12 * nside * nside))
     ref = O.sht(f, nside, L, M)
-    sht = hpx.SHTCUDA(nside, lmax=L, mmax=M, precision=prec)
+    sht = hpx.SHTCUDA(nside, lmax=L, mmax=M, precision=prec, legendre_table=tab)
     a = sht(torch.from_numpy(f).float().to(cuda))
-    hpx.get_plan(nside, L, M, "ring", prec, 0).check()
+    plan = hpx.get_plan(nside, L, M, "ring", prec, 0, 64, tab)
+    plan.check()
+    assert (plan.table_bytes > 0) == tab
     e = rel(a, ref)
     print(f"{prec} forward nside={nside} L={L} M={M}: {e:.2e}")
     assert e < TOL[prec]
@@ -62,15 +65,16 @@ def test_tc_forward(hpx, cuda, nside, L, M, prec):
     assert torch.count_nonzero(a[:, torch.from_numpy(mask).to(cuda)]) == 0
 
 
+@pytest.mark.parametrize("tab", [True, False], ids=["table", "otf"])
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("nside,L,M", TC_CASES)
-def test_tc_inverse(hpx, cuda, nside, L, M, prec):
+def test_tc_inverse(hpx, cuda, nside, L, M, prec, tab):
     rng = np.random.default_rng(7 * nside + L + M)
     a = rand_alm(rng, L, M, (3,))
     ref = O.isht(a, nside)
-    isht = hpx.iSHTCUDA(nside, lmax=L, mmax=M, precision=prec)
+    isht = hpx.iSHTCUDA(nside, lmax=L, mmax=M, precision=prec, legendre_table=tab)
     f = isht(torch.from_numpy(a).to(torch.complex64).to(cuda))
-    hpx.get_plan(nside, L, M, "ring", prec, 0).check()
+    hpx.get_plan(nside, L, M, "ring", prec, 0, 64, tab).check()
     e = rel(f, ref)
     print(f"{prec} inverse nside={nside} L={L} M={M}: {e:.2e}")
     assert e < TOL[prec]
@@ -86,9 +90,10 @@ def test_tc_batch_not_multiple_of_64(hpx, cuda, prec):
     assert rel(a, O.sht(f, nside, L, L)) < TOL[prec]
 
 
+@pytest.mark.parametrize("tab", [True, False], ids=["table", "otf"])
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("k", [1, 2])
-def test_tc_refined_matches_fp64_refined(hpx, cuda, k, prec):
+def test_tc_refined_matches_fp64_refined(hpx, cuda, k, prec, tab):
     nside, L = 32, 63
     rng = np.random.default_rng(10 + k)
     a_true = rand_alm(rng, L, L, (2,), decay=1.0)
@@ -96,7 +101,7 @@ def test_tc_refined_matches_fp64_refined(hpx, cuda, k, prec):
     ref = O.sht(fmap, nside, L, L)
     for _ in range(k):
         ref = ref + O.sht(fmap - O.isht(ref, nside), nside, L, L)
-    sht = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, refine_iters=k)
+    sht = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, refine_iters=k, legendre_table=tab)
     out = sht(torch.from_numpy(fmap).float().to(cuda))
     e = rel(out, ref)
     print(f"{prec} refined k={k}: {e:.2e}")
@@ -140,3 +145,18 @@ def test_f16x3_per_map_scale(hpx, cuda):
         else:
             assert rel(g[i] / s, gref[i]) < 2e-6, i
     hpx.get_plan(nside, L, L, "ring", "f16x3", 0).check()
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_table_matches_on_the_fly(hpx, cuda, prec):
+    """Resident-table and on-the-fly Pbar give the same transforms up to the
+    FP32 rounding of Pbar (the two round at different points)."""
+    rng = np.random.default_rng(11)
+    nside, L = 64, 127
+    f = torch.from_numpy(rng.standard_normal((3, 12 * nside * nside))).float().to(cuda)
+    at = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=True)(f)
+    ao = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=False)(f)
+    assert rel(at, ao.cpu().numpy()) < 1e-6
+    gt = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=True)(at)
+    go = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=False)(at)
+    assert rel(gt, go.cpu().numpy()) < 1e-6
