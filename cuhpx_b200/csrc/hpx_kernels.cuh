@@ -290,7 +290,8 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
         if (j < h) chirp[rp.gtab_off + j] = {(T)v.re, (T)(-v.im)};
     }
     __syncthreads();
-    cplx<double>* r = stockham<double, false>(buf, buf2, rp.logP, twP, threadIdx.x, blockDim.x, 0);
+    cplx<double>* r = fft_pow2<double, false>(buf, buf2, rp.logP, twP, threadIdx.x, blockDim.x, 0, IdentityMap{},
+                                              IdentityMap{});
     const double inv = 1.0 / (double)P;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         gtab[rp.gtab_off + j] = {(T)(r[padi(j)].re * inv), (T)(r[padi(j)].im * inv)};

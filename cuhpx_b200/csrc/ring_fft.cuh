@@ -115,79 +115,131 @@ __device__ __forceinline__ void dft16(cplx<T>* v) {
     for (int i = 0; i < 16; ++i) v[i] = o[i];
 }
 
-// Stockham autosort FFT of length P = 2^logP on src (natural order); returns the
-// buffer (src or dst) holding the natural-order result.  twP[q] = e^{-2 pi i q/P}
-// for q < P/2 (shared memory).  INV: e^{+2 pi i jk/P} (unnormalised).
-// First pass radix-16 in registers (contiguous 16-element stores), then radix-4
-// stages, and one radix-2 stage when log2(P) is odd.
+// 8-point DFT in registers: two 4-point DFTs of the even and odd samples and
+// the factors W8^k.
 template <typename T, bool INV>
-__device__ cplx<T>* stockham(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt,
-                             int tpf, int g) {
+__device__ __forceinline__ void dft8(cplx<T>* v) {
+    cplx<T> e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    cplx<T> o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<T, INV>(e0, e1, e2, e3);
+    dft4<T, INV>(o0, o1, o2, o3);
+    const T r = (T)0.70710678118654752440;
+    const T sg = INV ? (T)1 : (T)-1;
+    o1 = cmul(o1, cplx<T>{r, sg * r});
+    o2 = cplx<T>{-sg * o2.im, sg * o2.re};  // times (0, sg)
+    o3 = cmul(o3, cplx<T>{-r, sg * r});
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1);
+    v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2);
+    v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3);
+    v[7] = csub(e3, o3);
+}
+
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void dftR(cplx<T>* v) {
+    if constexpr (R == 2) {
+        const cplx<T> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        dft4<T, INV>(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 8) {
+        dft8<T, INV>(v);
+    } else {
+        dft16<T, INV>(v);
+    }
+}
+
+// One Stockham pass of radix R over a length-P sequence whose first Ns-point
+// sub-transforms are done: inputs src[j + rQ] (Q = P/R), outputs dst[o + r Ns]
+// with o = (j mod Ns) + R (j - j mod Ns).  Twiddles e^{-/+2 pi i r k/(Ns R)}
+// are read from twP (q < P/2) with e^{-2 pi i (q + P/2)/P} = -twP[q], never
+// built by repeated multiplication.  The first pass maps its inputs through
+// pre(i, v) (natural index i), the last pass its outputs through post(i, v).
+template <typename T, bool INV, int R, bool FIRST, bool LAST, typename Pre, typename Post>
+__device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P, int Ns,
+                                         const cplx<T>* __restrict__ twP, int lt, int tpf, Pre& pre, Post& post) {
+    const int Q = P / R;
+    const int step = P / (Ns * R);
+    const int half = P >> 1;
+    for (int j = lt; j < Q; j += tpf) {
+        const int k = j & (Ns - 1);
+        cplx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            v[r] = src[padi(j + r * Q)];
+            if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
+        }
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const int q = r * k * step;
+                cplx<T> w = q < half ? twP[q] : cplx<T>{-twP[q - half].re, -twP[q - half].im};
+                if (INV) w.im = -w.im;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        dftR<T, INV, R>(v);
+        const int o = ((j - k) * R) + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cplx<T> x = v[r];
+            if constexpr (LAST) x = post(o + r * Ns, x);
+            dst[padi(o + r * Ns)] = x;
+        }
+    }
+}
+
+struct IdentityMap {
+    template <typename V>
+    __device__ __forceinline__ V operator()(int, V v) const { return v; }
+};
+
+// Stockham autosort FFT of length P = 2^logP (logP >= 1) on src (natural
+// order, padded indexing); returns the buffer (src or dst) holding the
+// natural-order result.  One radix-2/4/8 pass for logP mod 4, then radix-16
+// passes: 3 passes for P = 4096.  twP[q] = e^{-2 pi i q/P}, q < P/2 (shared).
+// INV: e^{+2 pi i jk/P} (unnormalised).  pre/post as in fft_pass.
+template <typename T, bool INV, typename Pre, typename Post>
+__device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
+                             int g, Pre pre, Post post) {
     const int P = 1 << logP;
-    int Ns = 1;
-    int rem = logP;
-    auto swap_bufs = [&]() {
+    const int n16 = logP >> 2, r0 = logP & 3;
+    const int npass = n16 + (r0 ? 1 : 0);
+    int Ns = 1, pass = 0;
+    auto next = [&]() {
         group_sync(tpf, g);
         cplx<T>* t = src;
         src = dst;
         dst = t;
+        ++pass;
     };
-    if (rem >= 4) {
-        const int Q = P >> 4;
-        for (int j = lt; j < Q; j += tpf) {
-            cplx<T> v[16];
-#pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = src[padi(j + r * Q)];
-            dft16<T, INV>(v);
-            // outputs 16j .. 16j+15 are one aligned 16-run: padded index 17j + r
-#pragma unroll
-            for (int r = 0; r < 16; ++r) dst[17 * j + r] = v[r];
+    if (r0) {
+        const bool last = npass == 1;
+        if (r0 == 1) {
+            if (last) fft_pass<T, INV, 2, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            else fft_pass<T, INV, 2, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        } else if (r0 == 2) {
+            if (last) fft_pass<T, INV, 4, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            else fft_pass<T, INV, 4, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        } else {
+            if (last) fft_pass<T, INV, 8, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            else fft_pass<T, INV, 8, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
         }
-        Ns = 16;
-        rem -= 4;
-        swap_bufs();
+        Ns <<= r0;
+        next();
     }
-    while (rem >= 2) {
-        const int Q = P >> 2;
-        const int step = P / (Ns * 4);
-        for (int j = lt; j < Q; j += tpf) {
-            const int k = j & (Ns - 1);
-            cplx<T> v0 = src[padi(j)], v1 = src[padi(j + Q)], v2 = src[padi(j + 2 * Q)], v3 = src[padi(j + 3 * Q)];
-            if (Ns > 1) {
-                cplx<T> w1 = twP[k * step];
-                if (INV) w1.im = -w1.im;
-                const cplx<T> w2 = cmul(w1, w1), w3 = cmul(w1, w2);
-                v1 = cmul(v1, w1);
-                v2 = cmul(v2, w2);
-                v3 = cmul(v3, w3);
-            }
-            dft4<T, INV>(v0, v1, v2, v3);
-            const int o = ((j - k) << 2) + k;
-            dst[padi(o)] = v0;
-            dst[padi(o + Ns)] = v1;
-            dst[padi(o + 2 * Ns)] = v2;
-            dst[padi(o + 3 * Ns)] = v3;
-        }
-        Ns <<= 2;
-        rem -= 2;
-        swap_bufs();
-    }
-    if (rem == 1) {
-        const int Q = P >> 1;
-        const int step = P / (Ns * 2);
-        for (int j = lt; j < Q; j += tpf) {
-            const int k = j & (Ns - 1);
-            cplx<T> v0 = src[padi(j)], v1 = src[padi(j + Q)];
-            if (Ns > 1) {
-                cplx<T> w = twP[k * step];
-                if (INV) w.im = -w.im;
-                v1 = cmul(v1, w);
-            }
-            const int o = ((j - k) << 1) + k;
-            dst[padi(o)] = cadd(v0, v1);
-            dst[padi(o + Ns)] = csub(v0, v1);
-        }
-        swap_bufs();
+    for (int i = 0; i < n16; ++i) {
+        const bool first = pass == 0, last = pass == npass - 1;
+        if (first && last) fft_pass<T, INV, 16, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        else if (first) fft_pass<T, INV, 16, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        else if (last) fft_pass<T, INV, 16, false, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        else fft_pass<T, INV, 16, false, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        Ns <<= 4;
+        next();
     }
     return src;
 }
@@ -227,37 +279,33 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp, bool inv, int lt,
                              int tpf, int g) {
     group_sync(tpf, g);
+    IdentityMap id;
     if (rp.logh >= 0) {
         if (rp.logh == 0) return buf;
-        return inv ? stockham<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g)
-                   : stockham<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g);
+        return inv ? fft_pow2<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id)
+                   : fft_pow2<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id);
     }
-    // Bluestein; inverse via conj(DFT(conj z)).  c_j = e^{-i pi j^2/h}.
-    const int P = 1 << rp.logP;
+    // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
+    // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
+    // (scaled by 1/P); the inverse transform is conj(DFT(conj z)).  The chirp
+    // products ride on the first loads and the last stores of the two FFTs.
     const int h = rp.h;
-    for (int j = lt; j < P; j += tpf) {
-        cplx<T> a = {(T)0, (T)0};
-        if (j < h) {
-            a = buf[padi(j)];
-            if (inv) a.im = -a.im;
-            a = cmul(a, chirp[j]);
-        }
-        buf[padi(j)] = a;
-    }
-    group_sync(tpf, g);
-    cplx<T>* r = stockham<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g);
-    cplx<T>* o = (r == buf) ? buf2 : buf;
     const cplx<T>* G = gtab + rp.gtab_off;
-    for (int j = lt; j < P; j += tpf) r[padi(j)] = cmul(r[padi(j)], G[j]);
-    group_sync(tpf, g);
-    r = stockham<T, true>(r, o, rp.logP, twP, lt, tpf, g);
-    for (int k = lt; k < h; k += tpf) {
-        cplx<T> v = cmul(r[padi(k)], chirp[k]);
+    auto pre = [&](int j, cplx<T> a) {
+        if (j >= h) return cplx<T>{(T)0, (T)0};
+        if (inv) a.im = -a.im;
+        return cmul(a, chirp[j]);
+    };
+    auto mulG = [&](int k, cplx<T> a) { return cmul(a, G[k]); };
+    auto postc = [&](int k, cplx<T> a) {
+        if (k >= h) return a;
+        cplx<T> v = cmul(a, chirp[k]);
         if (inv) v.im = -v.im;
-        r[padi(k)] = v;
-    }
-    group_sync(tpf, g);
-    return r;
+        return v;
+    };
+    cplx<T>* r = fft_pow2<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
+    cplx<T>* o = (r == buf) ? buf2 : buf;
+    return fft_pow2<T, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
 }
 
 // Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
