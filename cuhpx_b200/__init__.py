@@ -6,7 +6,10 @@ C ABI in ``include/hpx_b200.h``); there is no CPU fallback.
 """
 
 from . import sht_tools
-from .hpx_sht import Plan, SHTCUDA, SHTFunction, clear_plan_cache, get_plan, iSHTCUDA, iSHTFunction
+from .hpx_sht import (LatLonPlan, Plan, SHTCUDA, SHTFunction, clear_plan_cache, get_latlon_plan, get_plan, iSHTCUDA,
+                      iSHTFunction)
+from .latlon import InverseRealSHT, RealSHT
+from .regrid import Grid, Regridding
 
 __all__ = [
     "SHTCUDA",
@@ -14,6 +17,12 @@ __all__ = [
     "SHTFunction",
     "iSHTFunction",
     "Plan",
+    "LatLonPlan",
+    "get_latlon_plan",
+    "RealSHT",
+    "InverseRealSHT",
+    "Grid",
+    "Regridding",
     "get_plan",
     "clear_plan_cache",
     "sht_tools",

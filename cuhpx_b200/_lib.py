@@ -26,6 +26,24 @@ FLAG_OTF_LEGENDRE = 1
 
 PRECISIONS = {"fp32": 0, "fp64": 1, "bf16x3": 2, "tf32": 3, "f16x3": 4}
 
+GRIDS = {"equiangular": 0, "legendre-gauss": 1, "lobatto": 2}
+
+
+class HpxLatLonDesc(ctypes.Structure):
+    _fields_ = [
+        ("nlat", ctypes.c_int32),
+        ("nlon", ctypes.c_int32),
+        ("lmax", ctypes.c_int32),
+        ("mmax", ctypes.c_int32),
+        ("grid", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("batch_chunk", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 # exported symbols and their signatures (argtypes, restype)
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
@@ -64,6 +82,7 @@ SIGNATURES = {
     "hpx_sht_forward_refined": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_noalloc": ([_vp, _vp, _vp, _i64, _vp], ctypes.c_int),
     "hpx_plan_table_bytes": ([_vp, ctypes.POINTER(_sz)], ctypes.c_int),
+    "hpx_plan_create_latlon": ([ctypes.POINTER(HpxLatLonDesc), ctypes.POINTER(_vp)], ctypes.c_int),
     "hpx_plan_info": (
         [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
         ctypes.c_int,

@@ -78,6 +78,24 @@ HPX_HD int first_ring_for_m(int m, int nside) {
     return t;
 }
 
+// ------------------------------------------------------------------ grid of rings
+// What the kernels need to know about the iso-latitude grid of a plan: NP
+// ring pairs (north ring p and its mirror), R rings, npix samples per map, and
+// which north rings carry order m.  HEALPix grids (nside > 0) truncate order m
+// to the rings with nphi/2 >= m; latitude-longitude grids (nside = 0) keep
+// orders m < mt_all on every ring.
+struct Geom {
+    int NP;
+    int R;
+    int64_t npix;
+    int nside;
+    int mt_all;
+    HPX_HD int first_ring(int m) const {
+        if (nside > 0) return first_ring_for_m(m, nside);
+        return m < mt_all ? 0 : NP;
+    }
+};
+
 // ------------------------------------------------------------------ complex
 template <typename T>
 struct __align__(2 * sizeof(T)) cplx {

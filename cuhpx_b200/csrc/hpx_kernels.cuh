@@ -17,13 +17,13 @@ __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
 // One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
 template <typename T>
 __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
-                                                  T* __restrict__ F, int64_t Ftot, int nside,
+                                                  T* __restrict__ F, int64_t Ftot, Geom geo,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
                                                   int logPmax, const cplx<T>* __restrict__ gtab,
                                                   const cplx<T>* __restrict__ chirp,
                                                   unsigned* __restrict__ fmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NP = 2 * nside, R = 4 * nside - 1;
+    const int NP = geo.NP, R = geo.R;
     const int t = blockIdx.x;
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
     const int64_t start = south ? rp.start_s : rp.start_n;
     const int64_t foff = south ? rp.foff_s : rp.foff_n;
     const int shift = south ? rp.shift_s : rp.shift_n;
-    const int64_t np = npix(nside);
+    const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
     for (int b = b0 + g; b < b1; b += S) {
@@ -63,12 +63,12 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
 // (ref != nullptr: write ref - synthesis)
 template <typename T>
 __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map,
-                                                  int nmaps, int maps_per_cta, int nside,
+                                                  int nmaps, int maps_per_cta, Geom geo,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
                                                   int logPmax, const cplx<T>* __restrict__ gtab,
                                                   const cplx<T>* __restrict__ chirp, const T* __restrict__ ref) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NP = 2 * nside, R = 4 * nside - 1;
+    const int NP = geo.NP, R = geo.R;
     const int t = blockIdx.x;
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64
     const int64_t start = south ? rp.start_s : rp.start_n;
     const int64_t foff = south ? rp.foff_s : rp.foff_n;
     const int shift = south ? rp.shift_s : rp.shift_n;
-    const int64_t np = npix(nside);
+    const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
     for (int b = b0 + g; b < b1; b += S)
@@ -133,14 +133,14 @@ template <typename T>
 constexpr int fold_mb() { return sizeof(T) == 4 ? 32 : 16; }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t Ftot, int nmaps, int nside,
+__global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t Ftot, int nmaps, Geom geo,
                                               const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ spec,
                                               int C, uint32_t* __restrict__ xh, uint32_t* __restrict__ xl,
                                               const unsigned* __restrict__ fmax, float wb) {
     constexpr int MB = fold_mb<T>();
     __shared__ cplx<T> tn[64][MB + 1];
     __shared__ cplx<T> ts[64][MB + 1];
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int m0 = blockIdx.x * MB, p = blockIdx.y, bz = blockIdx.z * 64;
     const RingPair rp = pairs[p];
     if (m0 >= rp.mt) return;
@@ -205,13 +205,13 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
 // into ring spectra F_t = sc (E + O), F_t' = sc (E - O), with sc = 1, or for
 // the adjoint of analysis sc = w_t (m = 0, nphi/2) and w_t/2 otherwise.
 template <typename T>
-__global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int C, int nmaps, int nside,
+__global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int C, int nmaps, Geom geo,
                                                 const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ F,
                                                 int64_t Ftot) {
     constexpr int MB = fold_mb<T>();
     __shared__ cplx<T> te[MB][65];
     __shared__ cplx<T> to[MB][65];
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int m0 = blockIdx.x * MB, p = blockIdx.y, bz = blockIdx.z * 64;
     const RingPair rp = pairs[p];
     if (m0 >= rp.mt) return;

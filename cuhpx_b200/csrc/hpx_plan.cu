@@ -76,7 +76,8 @@ const char* kStageNames[kNumStages] = {"ring_fft_forward", "ring_fft_inverse", "
 struct hpx_plan_s {
     hpx_desc_t desc{};
     int device = 0;
-    int nside = 0, L = 0, M = 0, NP = 0, R = 0;
+    int nside = 0, L = 0, M = 0, NP = 0, R = 0;  // nside = 0: latitude-longitude grid
+    Geom geo{};
     int64_t npix = 0;
     int prec = HPX_PREC_FP32;
     bool f64 = false;
@@ -304,10 +305,10 @@ int tc_table_create(hpx_plan_s* P) {
     const int64_t n = (int64_t)T.m_tc_end * seed_blocks(P->L) * P->NP;
     const unsigned grid = (unsigned)((n + 127) / 128);
     if (P->f16())
-        k_legendre_table<true><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->nside, T.Lt, P->d_z, P->d_lstart,
+        k_legendre_table<true><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->geo, T.Lt, P->d_z, P->d_lstart,
                                               P->d_pstart, P->d_coef, P->d_seeds, T.d_table);
     else
-        k_legendre_table<false><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->nside, T.Lt, P->d_z, P->d_lstart,
+        k_legendre_table<false><<<grid, 128>>>(T.m_tc_end, P->L, P->Lpad, P->geo, T.Lt, P->d_z, P->d_lstart,
                                                P->d_pstart, P->d_coef, P->d_seeds, T.d_table);
     HPX_CUDA_TRY(cudaGetLastError());
     HPX_CUDA_TRY(cudaDeviceSynchronize());
@@ -333,15 +334,14 @@ int tc_create(hpx_plan_s* P) {
     HPX_CUDA_TRY(cudaDeviceGetAttribute(&T.nsm, cudaDevAttrMultiProcessorCount, P->device));
     HPX_CUDA_TRY(cudaMalloc(&T.d_err, sizeof(int)));
     HPX_CUDA_TRY(cudaMemset(T.d_err, 0, sizeof(int)));
-    const int N = P->nside;
-    T.m_tc_end = std::min(std::min(P->L, P->M), 2 * N + 1);
+    T.m_tc_end = std::min(std::min(P->L, P->M), P->mtmax);
     T.Lh = (P->L + 65) / 2;
     const int rc = tc_table_create(P);
     if (rc != HPX_OK) return rc;
     std::vector<int2> ft, it;
     for (int m = 0; m < T.m_tc_end; ++m) {
         for (int j = 0; j < (P->L - m + kTcFwdDeg - 1) / kTcFwdDeg; ++j) ft.push_back(make_int2(m, j));
-        const int K = P->NP - first_ring_for_m(m, N);
+        const int K = P->NP - P->geo.first_ring(m);
         for (int rb = 0; rb < K; rb += kTcInvRings) it.push_back(make_int2(m, rb));
     }
     T.n_fwd_tiles = (int)ft.size();
@@ -355,7 +355,7 @@ int tc_create(hpx_plan_s* P) {
     const double kSlow = T.table ? 1.0 : 2.0, kTileFixed = 7.0;
     std::vector<double> fc, ic;
     for (const int2& t : ft) {
-        const int nch = (P->NP - first_ring_for_m(t.x, N) + kFRing - 1) / kFRing;
+        const int nch = (P->NP - P->geo.first_ring(t.x) + kFRing - 1) / kFRing;
         fc.push_back(nch * (t.x + t.y * kTcFwdDeg < P->h_lsmax[t.x] ? kSlow : 1.0) + kTileFixed);
     }
     for (const int2& t : it) {
@@ -415,42 +415,167 @@ __global__ void k_zero_alm_cols(float* __restrict__ alm, int nmaps, int L, int M
     }
 }
 
-int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
+// Common plan fields from the descriptor (geometry set by the caller).
+void plan_init(const hpx_desc_t* d, hpx_plan_s* P) {
     P->desc = *d;
     P->desc.ring_weights = nullptr;
     P->device = d->device;
     P->nside = d->nside;
     P->L = d->lmax;
     P->M = d->mmax;
-    P->NP = 2 * d->nside;
-    P->R = 4 * d->nside - 1;
-    P->npix = 12ll * d->nside * d->nside;
     P->prec = d->precision;
     P->f64 = d->precision == HPX_PREC_FP64;
     P->batch_chunk = d->batch_chunk > 0 ? d->batch_chunk : 64;
-    const int N = P->nside;
+}
 
-    // ---- ring pairs
+// HEALPix ring pairs (RING order, cuhpx/sht_tools.py:114-189, 319-332):
+// north ring p = t and its mirror 4N-2-p; the equator pairs with itself.
+void healpix_pairs(const hpx_desc_t* d, hpx_plan_s* P) {
+    const int N = d->nside;
+    P->NP = 2 * N;
+    P->R = 4 * N - 1;
+    P->npix = 12ll * N * N;
+    P->geo = Geom{P->NP, P->R, P->npix, N, 0};
     P->h_pairs.resize(P->NP);
-    int64_t goff = 0;
-    int logPmax = 1, bufP = 2, mtmax = 0;
     const double four_pi_over_npix = 4.0 * M_PI / (double)P->npix;
     for (int p = 0; p < P->NP; ++p) {
         RingPair& rp = P->h_pairs[p];
         std::memset(&rp, 0, sizeof(rp));
         const int ts = 4 * N - 2 - p;
         rp.nphi = ring_nphi(p, N);
-        rp.h = rp.nphi / 2;
-        rp.mt = std::min(P->M, rp.h + 1);
         rp.shift_n = ring_shift(p, N);
         rp.shift_s = ring_shift(ts, N);
         rp.has_south = p != 2 * N - 1;
         rp.start_n = ring_start(p, N);
         rp.start_s = ring_start(ts, N);
         rp.z = ring_z(p, N);
+        rp.s2 = ring_sin2(p, N);
         // quadrature weight (cuhpx/sht_tools.py:47-59): north ring index p+1
         if (d->ring_weights) rp.w = four_pi_over_npix * (1.0 + d->ring_weights[p]);
         else rp.w = four_pi_over_npix;
+    }
+}
+
+// Latitude-longitude ring pairs: nlat rings of nlon samples each, phi_k =
+// 2 pi k / nlon, ring t at cos(theta_t) = z[t] with quadrature weight w[t]
+// (the nodes mirror: z[nlat-1-t] = -z[t]); the ring weight carries the
+// longitude factor 2 pi / nlon.
+void latlon_pairs(int nlat, int nlon, const std::vector<double>& z, const std::vector<double>& s2,
+                  const std::vector<double>& w, hpx_plan_s* P) {
+    P->NP = (nlat + 1) / 2;
+    P->R = nlat;
+    P->npix = (int64_t)nlat * nlon;
+    P->geo = Geom{P->NP, P->R, P->npix, 0, std::min(P->M, nlon / 2 + 1)};
+    P->h_pairs.resize(P->NP);
+    for (int p = 0; p < P->NP; ++p) {
+        RingPair& rp = P->h_pairs[p];
+        std::memset(&rp, 0, sizeof(rp));
+        const int ts = nlat - 1 - p;
+        rp.nphi = nlon;
+        rp.has_south = ts != p;
+        rp.start_n = (int64_t)p * nlon;
+        rp.start_s = (int64_t)ts * nlon;
+        rp.z = z[p];
+        rp.s2 = s2[p];
+        rp.w = w[p] * 2.0 * M_PI / (double)nlon;
+    }
+}
+
+// Quadrature nodes z_j = cos(theta_j) (north to south), sin^2(theta_j) and
+// weights (summing to 2) of a latitude-longitude grid, in FP64.
+void latlon_quadrature(int grid, int n, std::vector<double>& z, std::vector<double>& s2, std::vector<double>& w) {
+    z.assign(n, 0.0);
+    s2.assign(n, 0.0);
+    w.assign(n, 0.0);
+    // P_k(x) and P_k'(x) by the three-term recurrence and P_j' = j P_{j-1} + x P_{j-1}'
+    // (no division by 1 - x^2, so accurate next to the poles)
+    auto legendre = [](int k, double x, double& pk, double& dpk) {
+        double p0 = 1.0, p1 = x, d1 = 1.0;
+        if (k == 0) {
+            pk = 1.0;
+            dpk = 0.0;
+            return;
+        }
+        for (int j = 2; j <= k; ++j) {
+            const double p2 = ((2.0 * j - 1.0) * x * p1 - (j - 1.0) * p0) / j;
+            d1 = j * p1 + x * d1;
+            p0 = p1;
+            p1 = p2;
+        }
+        pk = p1;
+        dpk = d1;
+    };
+    if (grid == HPX_GRID_EQUIANGULAR) {
+        // Clenshaw-Curtis on theta_j = pi j / N, N = n - 1
+        const int N = n - 1;
+        for (int j = 0; j < n; ++j) {
+            const double th = M_PI * j / N;
+            double sum = 0.0;
+            for (int k = 1; 2 * k <= N; ++k) {
+                const double b = (2 * k == N) ? 1.0 : 2.0;
+                sum += b / (4.0 * k * k - 1.0) * std::cos(2.0 * k * th);
+            }
+            const double c = (j == 0 || j == N) ? 1.0 : 2.0;
+            w[j] = c / N * (1.0 - sum);
+            z[j] = std::cos(th);
+            const double st = std::sin(th);
+            s2[j] = st * st;
+        }
+        z[0] = 1.0;
+        z[N] = -1.0;
+        s2[0] = s2[N] = 0.0;
+    } else if (grid == HPX_GRID_LEGENDRE_GAUSS) {
+        for (int i = 0; i < (n + 1) / 2; ++i) {
+            double x = std::cos(M_PI * (i + 0.75) / (n + 0.5)), pk = 0, dpk = 0;
+            for (int it = 0; it < 100; ++it) {
+                legendre(n, x, pk, dpk);
+                const double dx = pk / dpk;
+                x -= dx;
+                if (std::fabs(dx) < 1e-16) break;
+            }
+            legendre(n, x, pk, dpk);
+            z[i] = x;
+            z[n - 1 - i] = -x;
+            w[i] = w[n - 1 - i] = 2.0 / ((1.0 - x * x) * dpk * dpk);
+        }
+        if (n & 1) z[n / 2] = 0.0;
+        for (int i = 0; i < n; ++i) s2[i] = (1.0 - z[i]) * (1.0 + z[i]);
+    } else {
+        // Lobatto: +-1 and the roots of P'_N, N = n - 1; w = 2 / (N (N+1) P_N^2)
+        const int N = n - 1;
+        for (int i = 0; i < (n + 1) / 2; ++i) {
+            double x = i == 0 ? 1.0 : std::cos(M_PI * i / N), pk = 0, dpk = 0;
+            if (i > 0) {
+                for (int it = 0; it < 100; ++it) {
+                    legendre(N, x, pk, dpk);
+                    // f = (1 - x^2) P_N', f' = -N (N+1) P_N
+                    const double dx = ((1.0 - x * x) * dpk) / (-(double)N * (N + 1) * pk);  // f / f'
+                    x -= dx;
+                    if (std::fabs(dx) < 1e-16) break;
+                }
+            }
+            legendre(N, x, pk, dpk);
+            if (i == 0) pk = 1.0;
+            z[i] = x;
+            z[n - 1 - i] = -x;
+            w[i] = w[n - 1 - i] = 2.0 / ((double)N * (N + 1) * pk * pk);
+        }
+        if (n & 1) z[n / 2] = 0.0;
+        for (int i = 0; i < n; ++i) s2[i] = (1.0 - z[i]) * (1.0 + z[i]);
+        s2[0] = s2[n - 1] = 0.0;
+    }
+}
+
+// Everything after the ring-pair table: FFT sizes, spectrum offsets, Legendre
+// start values, seeds and coefficient tables, work lists, FFT tables and the
+// tensor-core state.
+int plan_build(hpx_plan_s* P) {
+    int64_t goff = 0;
+    int logPmax = 1, bufP = 2, mtmax = 0, nmax = 1;
+    for (int p = 0; p < P->NP; ++p) {
+        RingPair& rp = P->h_pairs[p];
+        rp.h = rp.nphi / 2;
+        rp.mt = std::min(P->M, rp.h + 1);
         rp.logh = ilog2_exact(rp.h);
         if (rp.logh >= 0) {
             rp.logP = rp.logh;
@@ -466,6 +591,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
         // threads per FFT: ~16 points per thread, between one warp and the CTA
         rp.tpf = std::min(256, std::max(32, Pf / 16));
         mtmax = std::max(mtmax, rp.mt);
+        nmax = std::max(nmax, rp.nphi);
         P->wmax = std::max(P->wmax, (float)rp.w);
     }
     // ring-major spectrum offsets: north rings 0..NP-1, then south rings
@@ -480,7 +606,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     P->logPmax = logPmax;
     P->bufP = bufP;
     P->mtmax = mtmax;
-    P->nmax = 4 * N;
+    P->nmax = nmax;
 
     HPX_CUDA_TRY(cudaMalloc(&P->d_pairs, sizeof(RingPair) * P->NP));
     HPX_CUDA_TRY(cudaMemcpy(P->d_pairs, P->h_pairs.data(), sizeof(RingPair) * P->NP, cudaMemcpyHostToDevice));
@@ -498,7 +624,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     const int64_t nms = (int64_t)P->M * P->NP;
     HPX_CUDA_TRY(cudaMalloc(&P->d_lstart, sizeof(int) * nms));
     HPX_CUDA_TRY(cudaMalloc(&P->d_pstart, sizeof(double2) * nms));
-    k_legendre_start<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, N, P->d_pairs, d_logc, P->d_lstart,
+    k_legendre_start<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, P->geo, P->d_pairs, d_logc, P->d_lstart,
                                                            P->d_pstart);
     cudaError_t e = cudaGetLastError();
     cudaError_t e2 = cudaDeviceSynchronize();
@@ -515,7 +641,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
         std::vector<int> hls((size_t)nms), hmax(P->M, 0);
         HPX_CUDA_TRY(cudaMemcpy(hls.data(), P->d_lstart, sizeof(int) * nms, cudaMemcpyDeviceToHost));
         for (int m = 0; m < P->M; ++m) {
-            const int t0 = first_ring_for_m(m, N);
+            const int t0 = P->geo.first_ring(m);
             int mx = m;
             for (int p = t0; p < P->NP; ++p) mx = std::max(mx, hls[(size_t)m * P->NP + p]);
             hmax[m] = mx;
@@ -543,7 +669,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     const size_t nseed = (size_t)P->M * seed_blocks(P->L) * P->NP;
     HPX_CUDA_TRY(cudaMalloc(&P->d_seeds, sizeof(double2) * nseed));
     HPX_CUDA_TRY(cudaMemset(P->d_seeds, 0, sizeof(double2) * nseed));
-    k_legendre_seeds<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, P->Lpad, N, P->d_pairs, P->d_lstart,
+    k_legendre_seeds<<<(unsigned)((nms + 127) / 128), 128>>>(P->M, P->L, P->Lpad, P->geo, P->d_pairs, P->d_lstart,
                                                            P->d_pstart, P->d_coef, P->d_seeds);
     e = cudaGetLastError();
     e2 = cudaDeviceSynchronize();
@@ -564,7 +690,7 @@ int plan_create(const hpx_desc_t* d, hpx_plan_s* P) {
     std::vector<int2> work;
     const int RBI = InvCfg<float>::RBI;
     for (int m = 0; m < P->M; ++m) {
-        const int t0 = first_ring_for_m(m, N);
+        const int t0 = P->geo.first_ring(m);
         const int K = P->NP - t0;
         for (int rb = 0; rb < K; rb += RBI) work.push_back(make_int2(m, rb));
     }
@@ -676,7 +802,7 @@ struct Pipeline {
             Timer tm(P, st, kStRingFwd);
             if (fmax) cudaMemsetAsync(fmax, 0, sizeof(unsigned) * nb, st);
             dim3 grid(P->R, (nb + g - 1) / g);
-            k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->nside, P->d_pairs,
+            k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->geo, P->d_pairs,
                                                           (const cplx<T>*)P->d_tw, P->logPmax,
                                                           (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, fmax);
         }
@@ -684,7 +810,7 @@ struct Pipeline {
         // |c (F_t +- F_t')| <= 2 max|c| max|F|: c = w_t, or c_m <= 2 for the adjoint
         fold_wb = adjoint ? 4.f : 2.f * P->wmax;
         dim3 fg((P->mtmax + fold_mb<T>() - 1) / fold_mb<T>(), P->NP, (nb + 63) / 64);
-        k_fold<T><<<fg, 256, 0, st>>>(F, P->Ftot, nb, P->nside, P->d_pairs, adjoint, spec, P->cols(), xh(), xl(),
+        k_fold<T><<<fg, 256, 0, st>>>(F, P->Ftot, nb, P->geo, P->d_pairs, adjoint, spec, P->cols(), xh(), xl(),
                                       fmax, fold_wb);
     }
     // synthesis output spec (E/O) -> ring spectra F -> map (ref: residual ref - map)
@@ -692,12 +818,12 @@ struct Pipeline {
         {
             Timer tm(P, st, kStUnfold);
             dim3 fg((P->mtmax + fold_mb<T>() - 1) / fold_mb<T>(), P->NP, (nb + 63) / 64);
-            k_unfold<T><<<fg, 256, 0, st>>>(spec, P->cols(), nb, P->nside, P->d_pairs, adjoint, F, P->Ftot);
+            k_unfold<T><<<fg, 256, 0, st>>>(spec, P->cols(), nb, P->geo, P->d_pairs, adjoint, F, P->Ftot);
         }
         const int g = maps_per_cta_ring();
         Timer tm(P, st, kStRingInv);
         dim3 grid(P->R, (nb + g - 1) / g);
-        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(F, P->Ftot, map, nb, g, P->nside, P->d_pairs,
+        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(F, P->Ftot, map, nb, g, P->geo, P->d_pairs,
                                                       (const cplx<T>*)P->d_tw, P->logPmax, (const cplx<T>*)P->d_gtab,
                                                       (const cplx<T>*)P->d_chirp, ref);
     }
@@ -716,7 +842,7 @@ struct Pipeline {
             auto kern = TP.table ? (P->f16() ? k_leg_fwd_tc<true, true> : k_leg_fwd_tc<false, true>)
                                  : (P->f16() ? k_leg_fwd_tc<true, false> : k_leg_fwd_tc<false, false>);
             kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(
-                mh, ml, TP.table ? TP.tab_fwd : mh, nb, yc, P->L, P->Lpad, P->nside, P->d_z, P->d_lstart,
+                mh, ml, TP.table ? TP.tab_fwd : mh, nb, yc, P->L, P->Lpad, P->geo, P->d_z, P->d_lstart,
                 P->d_lsmax, P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, fmax,
                 fold_wb, TP.d_err);
             dim3 tg((TP.m_tc_end + 31) / 32, P->L);
@@ -724,7 +850,7 @@ struct Pipeline {
             return;
         }
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
-        k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->nside, P->d_pairs,
+        k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->geo, P->d_pairs,
                                                           P->d_lstart, P->d_pstart, P->d_coef, P->Lpad, P->d_seeds,
                                                           P->d_fwdtiles, accumulate);
     }
@@ -757,7 +883,7 @@ struct Pipeline {
             auto kern = TP.table ? (P->f16() ? k_leg_inv_tc<true, true> : k_leg_inv_tc<false, true>)
                                  : (P->f16() ? k_leg_inv_tc<true, false> : k_leg_inv_tc<false, false>);
             kern<<<TP.n_inv_ctas, kTcThreads, kISmem, st>>>(
-                mh, ml, TP.table ? TP.tab_inv : mh, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->nside, P->d_z, P->d_lstart, P->d_lsmax,
+                mh, ml, TP.table ? TP.tab_inv : mh, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->geo, P->d_z, P->d_lstart, P->d_lsmax,
                 P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.d_inv_off, amax, TP.d_err);
             return;
         }
@@ -769,7 +895,7 @@ struct Pipeline {
         Timer tm(P, st, kStLegInv);
         if (P->n_invwork == 0) return;
         dim3 grid(P->n_invwork, (C + InvCfg<T>::CT - 1) / InvCfg<T>::CT);
-        k_leg_inv_simt<T><<<grid, 256, P->inv_smem, st>>>(almT, C, spec, P->L, P->M, P->nside, P->d_pairs,
+        k_leg_inv_simt<T><<<grid, 256, P->inv_smem, st>>>(almT, C, spec, P->L, P->M, P->geo, P->d_pairs,
                                                           P->d_lstart, P->d_pstart, P->d_coef, P->Lpad,
                                                           P->d_invwork);
     }
@@ -956,7 +1082,61 @@ int hpx_plan_create(const hpx_desc_t* desc, hpx_plan_t* plan) {
     DeviceGuard g(desc->device);
     int rc;
     try {
-        rc = plan_create(desc, P);
+        plan_init(desc, P);
+        healpix_pairs(desc, P);
+        rc = plan_build(P);
+    } catch (const std::bad_alloc&) {
+        rc = set_err(HPX_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& ex) {
+        rc = set_err(HPX_ERR_CUDA, ex.what());
+    }
+    if (rc != HPX_OK) {
+        delete P;
+        return rc;
+    }
+    *plan = P;
+    return HPX_OK;
+}
+
+int hpx_plan_create_latlon(const hpx_latlon_desc_t* desc, hpx_plan_t* plan) {
+    if (!desc || !plan) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    *plan = nullptr;
+    if (desc->nlat < 2 || desc->nlat > 16384) return set_err(HPX_ERR_INVALID_ARG, "nlat must be in [2, 16384]");
+    if (desc->nlon < 2 || desc->nlon > 32768 || (desc->nlon & 1))
+        return set_err(HPX_ERR_INVALID_ARG, "nlon must be even and in [2, 32768]");
+    if (desc->lmax < 1 || desc->mmax < 1 || desc->lmax > 65536 || desc->mmax > 65536)
+        return set_err(HPX_ERR_INVALID_ARG, "lmax and mmax must be in [1, 65536]");
+    if (desc->grid < HPX_GRID_EQUIANGULAR || desc->grid > HPX_GRID_LOBATTO)
+        return set_err(HPX_ERR_INVALID_ARG, "unknown grid");
+    if (desc->precision < HPX_PREC_FP32 || desc->precision > HPX_PREC_F16X3)
+        return set_err(HPX_ERR_INVALID_ARG, "unknown precision");
+    if (desc->batch_chunk < 0 || desc->batch_chunk > 4096) return set_err(HPX_ERR_INVALID_ARG, "batch_chunk out of range");
+    if ((desc->flags & ~HPX_FLAG_OTF_LEGENDRE) || desc->reserved != 0)
+        return set_err(HPX_ERR_INVALID_ARG, "unknown flag bits");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_err(HPX_ERR_CUDA, "no CUDA device");
+    }
+    if (desc->device < 0 || desc->device >= ndev) return set_err(HPX_ERR_INVALID_ARG, "bad device ordinal");
+    hpx_plan_s* P = new (std::nothrow) hpx_plan_s();
+    if (!P) return set_err(HPX_ERR_OOM, "host allocation failed");
+    DeviceGuard g(desc->device);
+    int rc;
+    try {
+        hpx_desc_t d{};
+        d.nside = 0;
+        d.lmax = desc->lmax;
+        d.mmax = desc->mmax;
+        d.precision = desc->precision;
+        d.batch_chunk = desc->batch_chunk;
+        d.device = desc->device;
+        d.flags = desc->flags;
+        plan_init(&d, P);
+        std::vector<double> z, s2, w;
+        latlon_quadrature(desc->grid, desc->nlat, z, s2, w);
+        latlon_pairs(desc->nlat, desc->nlon, z, s2, w, P);
+        rc = plan_build(P);
     } catch (const std::bad_alloc&) {
         rc = set_err(HPX_ERR_OOM, "host allocation failed");
     } catch (const std::exception& ex) {

@@ -40,19 +40,19 @@ constexpr double kSeedLog2Floor = -1000.0;
 
 // Start values of the recurrence for (m, north ring p); see file comment.
 // logc[m] = log2(Pbar_m^m / sin^m(theta)) = log2(1/sqrt(4pi)) + 0.5 sum_k log2((2k+1)/(2k)).
-__global__ void k_legendre_start(int M, int L, int nside, const RingPair* __restrict__ pairs,
+__global__ void k_legendre_start(int M, int L, Geom geo, const RingPair* __restrict__ pairs,
                                  const double* __restrict__ logc, int* __restrict__ lstart,
                                  double2* __restrict__ pstart) {
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)M * NP) return;
     const int m = (int)(idx / NP), p = (int)(idx % NP);
     int ls = L;
     double2 ps = make_double2(0.0, 0.0);
-    if (m < L && p >= first_ring_for_m(m, nside)) {
+    const double s2 = pairs[p].s2;
+    if (m < L && p >= geo.first_ring(m) && (m == 0 || s2 > 0.0)) {  // poles carry m = 0 only
         const double x = pairs[p].z;
-        const double s2 = ring_sin2(p, nside);
-        const double lg = logc[m] + 0.5 * (double)m * log2(s2);
+        const double lg = m == 0 ? logc[0] : logc[m] + 0.5 * (double)m * log2(s2);
         // scaled pair: value = mant * 2^E
         double E = floor(lg);
         double q0 = exp2(lg - E);
@@ -110,10 +110,10 @@ constexpr int kSeedBlock = 64;
 
 __host__ __device__ inline int seed_blocks(int L) { return (L + kSeedBlock - 1) / kSeedBlock; }
 
-__global__ void k_legendre_seeds(int M, int L, int Lpad, int nside, const RingPair* __restrict__ pairs,
+__global__ void k_legendre_seeds(int M, int L, int Lpad, Geom geo, const RingPair* __restrict__ pairs,
                                  const int* __restrict__ lstart, const double2* __restrict__ pstart,
                                  const double2* __restrict__ coef, double2* __restrict__ seeds) {
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)M * NP) return;
     const int m = (int)(idx / NP), p = (int)(idx % NP);
@@ -214,7 +214,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec, int C, int nmaps,
-                                                      T* __restrict__ alm, int L, int M, int nside,
+                                                      T* __restrict__ alm, int L, int M, Geom geo,
                                                       const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
                                                       const double2* __restrict__ pstart,
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec
     constexpr int LT = Cfg::LT, CT = Cfg::CT, RB = Cfg::RB, KC = Cfg::KC, LTP = Cfg::LTP;
     constexpr int VPR = CT * sizeof(T) / 16;  // 16-byte vectors per staged row
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int2 tl = tiles[blockIdx.x];
     const int m = tl.x, jb = tl.y;
     const int l0 = m + jb * LT;
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec
     T* Pt = (T*)(cf + LT);
     T* Xs = Pt + RB * LTP;  // [2][KC][2][CT]
 
-    const int t0 = first_ring_for_m(m, nside);
+    const int t0 = geo.first_ring(m);
     const int K = NP - t0;
     const int nbk = seed_blocks(L);
 
@@ -393,7 +393,7 @@ __host__ __device__ constexpr size_t inv_smem_bytes(int L) {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT, int C, T* __restrict__ spec, int L,
-                                                      int M, int nside, const RingPair* __restrict__ pairs,
+                                                      int M, Geom geo, const RingPair* __restrict__ pairs,
                                                       const int* __restrict__ lstart,
                                                       const double2* __restrict__ pstart,
                                                       const double2* __restrict__ coef, int Lpad,
@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
     using Cfg = InvCfg<T>;
     constexpr int RBI = Cfg::RBI, CT = Cfg::CT, LC = Cfg::LC, RBP = Cfg::RBP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int2 wk = work[blockIdx.x];
     const int m = wk.x, rb = wk.y;
     const int c0 = blockIdx.y * CT;
@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
     T* Pt = (T*)(coefB + L);  // [LC][RBP], 16-byte aligned (2L doubles precede it)
     T* As = Pt + LC * RBP;                                          // [LC][CT]
 
-    const int t0 = first_ring_for_m(m, nside);
+    const int t0 = geo.first_ring(m);
     const int K = NP - t0;
 
     for (int l = m + 2 + tid; l < L; l += blockDim.x) {

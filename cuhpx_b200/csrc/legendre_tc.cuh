@@ -295,12 +295,12 @@ __device__ __forceinline__ void gen1_slow(int chain, int m, int l0b, int L, int 
 // Entries never written (rings before the first ring of m, degrees >= L)
 // must be zero: the caller clears the table first.
 template <bool F16>
-__global__ void __launch_bounds__(128) k_legendre_table(int m_end, int L, int Lpad, int nside, int Lt,
+__global__ void __launch_bounds__(128) k_legendre_table(int m_end, int L, int Lpad, Geom geo, int Lt,
                                                         const double* __restrict__ zr, const int* __restrict__ lstart,
                                                         const double2* __restrict__ pstart,
                                                         const double2* __restrict__ coef,
                                                         const double2* __restrict__ seeds, uint16_t* __restrict__ tab) {
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int nbk = seed_blocks(L);
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)m_end * nbk * NP) return;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(128) k_legendre_table(int m_end, int L, int Lp
     const int j = (int)((idx / NP) % nbk);
     const int m = (int)(idx / ((int64_t)NP * nbk));
     const int l0 = m + j * kSeedBlock;
-    if (l0 >= L || p < first_ring_for_m(m, nside)) return;
+    if (l0 >= L || p < geo.first_ring(m)) return;
     const int64_t mi = (int64_t)m * NP + p;
     const int ls = lstart[mi];
     const double2 ps = pstart[mi];
@@ -378,7 +378,7 @@ template <bool F16, bool TAB>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_fwd_tc(const __grid_constant__ CUtensorMap xh_map, const __grid_constant__ CUtensorMap xl_map,
                  const __grid_constant__ CUtensorMap tab_map, int nmaps,
-                 float* __restrict__ ycols, int L, int Lpad, int nside, const double* __restrict__ zr,
+                 float* __restrict__ ycols, int L, int Lpad, Geom geo, const double* __restrict__ zr,
                  const int* __restrict__ lstart, const int* __restrict__ lsmax, const double2* __restrict__ pstart,
                  const double2* __restrict__ coef, const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds,
                  const int2* __restrict__ tiles, const int* __restrict__ tile_off, const unsigned* __restrict__ fmax,
@@ -391,13 +391,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     AlphaC* coef_s = (AlphaC*)(base + kFStages * kFStageBytes);
     TcShared* sh = (TcShared*)(base + kFStages * kFStageBytes + 8 * kFCoef * 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int nbk = seed_blocks(L);
     const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, fmax, wb, nmaps);
     tc_setup(sh, kFStages, 1, warp);
     const uint32_t tmem = sh->tmem_base;
-    auto nchunks = [&](int m) { return (NP - first_ring_for_m(m, nside) + kFRing - 1) / kFRing; };
+    auto nchunks = [&](int m) { return (NP - geo.first_ring(m) + kFRing - 1) / kFRing; };
 
     if (warp == 0) {
         if (lane == 0) {
@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
                 const int m = tiles[t].x, jb = tiles[t].y;
-                const int t0 = first_ring_for_m(m, nside);
+                const int t0 = geo.first_ring(m);
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kFStages;
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int2 tt = tiles[t];
                 m = tt.x;
                 jb = tt.y;
-                t0 = first_ring_for_m(m, nside);
+                t0 = geo.first_ring(m);
                 nch = nchunks(m);
             }
         };
@@ -665,7 +665,7 @@ template <bool F16, bool TAB>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_inv_tc(const __grid_constant__ CUtensorMap ah_map, const __grid_constant__ CUtensorMap al_map,
                  const __grid_constant__ CUtensorMap tab_map,
-                 float* __restrict__ spec, int C, int nmaps, int L, int M, int Lpad, int nside,
+                 float* __restrict__ spec, int C, int nmaps, int L, int M, int Lpad, Geom geo,
                  const double* __restrict__ zr, const int* __restrict__ lstart, const int* __restrict__ lsmax,
                  const double2* __restrict__ pstart, const double2* __restrict__ coef,
                  const AlphaC* __restrict__ alphac, const double2* __restrict__ seeds, const int2* __restrict__ tiles,
@@ -678,7 +678,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     AlphaC* coef_s = (AlphaC*)(base + kIStages * kIStageBytes);
     TcShared* sh = (TcShared*)(base + kIStages * kIStageBytes + 8 * 64 * 16);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NP = 2 * nside;
+    const int NP = geo.NP;
     const int nbk = seed_blocks(L);
     const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, amax, 1.f, nmaps);
@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
                 const int m = tiles[t].x, rb = tiles[t].y;
-                const int t0 = first_ring_for_m(m, nside);
+                const int t0 = geo.first_ring(m);
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
                     const int s = it % kIStages;
@@ -778,7 +778,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, rb = tiles[t].y;
-            const int t0 = first_ring_for_m(m, nside);
+            const int t0 = geo.first_ring(m);
             const int rr = rb + ew * 32 + lane;
             const int p = t0 + rr;
             TCP_T0(e0);
@@ -826,7 +826,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int2 tt = tiles[t];
                 m = tt.x;
                 rb = tt.y;
-                t0 = first_ring_for_m(m, nside);
+                t0 = geo.first_ring(m);
                 nch = nchunks(m);
             }
         };

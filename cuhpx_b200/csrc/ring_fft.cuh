@@ -49,6 +49,7 @@ struct RingPair {
     int64_t gtab_off;  // offset of the chirp spectrum / chirp (complex elements), -1 if direct
     double z;          // cos(theta) of the north ring
     double w;          // quadrature weight of the ring
+    double s2;         // sin^2(theta) of the north ring (no cancellation near the poles)
 };
 
 // FFT work buffers are padded by one element every 16 so that the strided

@@ -149,7 +149,7 @@ class Plan:
         self._check_alm(a)
         B = a.shape[0]
         out = torch.empty((B, self.npix), dtype=self.dtype, device=a.device)
-        self._call(self._lib.hpx_sht_inverse, torch.view_as_real(a), out, B)
+        self._call(self._lib.hpx_sht_inverse, torch.view_as_real(a.resolve_conj().contiguous()), out, B)
         return out
 
     def forward_adjoint(self, g):
@@ -157,7 +157,7 @@ class Plan:
         self._check_alm(g)
         B = g.shape[0]
         out = torch.empty((B, self.npix), dtype=self.dtype, device=g.device)
-        self._call(self._lib.hpx_sht_forward_adjoint, torch.view_as_real(g), out, B)
+        self._call(self._lib.hpx_sht_forward_adjoint, torch.view_as_real(g.resolve_conj().contiguous()), out, B)
         return out
 
     def inverse_adjoint(self, g):
@@ -167,6 +167,50 @@ class Plan:
         out = torch.empty((B, self.lmax, self.mmax), dtype=self.cdtype, device=g.device)
         self._call(self._lib.hpx_sht_inverse_adjoint, g, torch.view_as_real(out), B)
         return out
+
+
+class LatLonPlan(Plan):
+    """An ``hpx_plan_t`` over a latitude-longitude grid (hpx_plan_create_latlon):
+    maps [B, nlat * nlon], rings north to south, same transform calls as Plan."""
+
+    def __init__(self, nlat, nlon, lmax, mmax, grid="equiangular", precision="fp32", device=0, batch_chunk=64,
+                 legendre_table=True):
+        lib = _lib.load()
+        if precision not in _lib.PRECISIONS:
+            raise ValueError(f"unknown precision {precision!r}; expected one of {sorted(_lib.PRECISIONS)}")
+        if grid not in _lib.GRIDS:
+            raise ValueError(f"unknown grid {grid!r}; expected one of {sorted(_lib.GRIDS)}")
+        self.nside = 0
+        self.nlat, self.nlon, self.grid = int(nlat), int(nlon), grid
+        self.lmax, self.mmax = int(lmax), int(mmax)
+        self.precision = precision
+        self.device = int(device)
+        self.dtype = torch.float64 if precision == "fp64" else torch.float32
+        self.cdtype = torch.complex128 if precision == "fp64" else torch.complex64
+        self.npix = self.nlat * self.nlon
+        desc = _lib.HpxLatLonDesc()
+        desc.nlat, desc.nlon, desc.lmax, desc.mmax = self.nlat, self.nlon, self.lmax, self.mmax
+        desc.grid = _lib.GRIDS[grid]
+        desc.precision = _lib.PRECISIONS[precision]
+        desc.batch_chunk = int(batch_chunk)
+        desc.device = self.device
+        desc.flags = 0 if legendre_table else _lib.FLAG_OTF_LEGENDRE
+        desc.reserved = 0
+        handle = ctypes.c_void_p()
+        _lib.check(lib.hpx_plan_create_latlon(ctypes.byref(desc), ctypes.byref(handle)))
+        self._h = handle
+        self._lib = lib
+
+
+def get_latlon_plan(nlat, nlon, lmax, mmax, grid, precision, device, batch_chunk=64, legendre_table=True):
+    key = ("latlon", int(nlat), int(nlon), int(lmax), int(mmax), grid, precision, int(device), int(batch_chunk),
+           bool(legendre_table))
+    with _plan_lock:
+        p = _plans.get(key)
+        if p is None:
+            p = LatLonPlan(nlat, nlon, lmax, mmax, grid, precision, device, batch_chunk, legendre_table)
+            _plans[key] = p
+        return p
 
 
 def get_plan(nside, lmax, mmax, quad_weights, precision, device, batch_chunk=64, legendre_table=True):

@@ -153,6 +153,33 @@ HPX_API int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stage
  * bounded pipeline wait since the last check (HPX_ERR_TIMEOUT, flag cleared). */
 HPX_API int hpx_plan_check(hpx_plan_t plan, void* stream);
 
+/* Latitude-longitude grids (the destination side of cuHPX's Regridding,
+ * cuhpx/hpx_regrid.py:21-91, which delegates it to torch_harmonics RealSHT /
+ * InverseRealSHT): nlat rings from north to south, nlon samples each at
+ * phi_k = 2 pi k / nlon, maps laid out [batch][nlat][nlon].  Nodes and
+ * quadrature weights (summing to 2 over cos(theta)):
+ *   EQUIANGULAR     theta_j = pi j / (nlat-1), poles included, Clenshaw-Curtis
+ *   LEGENDRE_GAUSS  Gauss-Legendre nodes (exact to degree 2 nlat - 1)
+ *   LOBATTO         Gauss-Lobatto nodes, poles included
+ * Analysis: a_lm = sum_j w_j Pbar_l^m(cos theta_j) (2 pi/nlon) sum_k f_jk
+ * e^{-i m phi_k}; synthesis as for HEALPix.  The orthonormal Pbar carry no
+ * Condon-Shortley phase (as the HEALPix transforms).  Plans from this entry
+ * point serve hpx_sht_forward/inverse and both adjoints. */
+typedef enum { HPX_GRID_EQUIANGULAR = 0, HPX_GRID_LEGENDRE_GAUSS = 1, HPX_GRID_LOBATTO = 2 } hpx_grid_t;
+typedef struct {
+    int32_t nlat;         /* rings, >= 2                                      */
+    int32_t nlon;         /* samples per ring, even, >= 2                     */
+    int32_t lmax;         /* number of degrees                                */
+    int32_t mmax;         /* number of orders (orders > nlon/2 are zero)      */
+    int32_t grid;         /* hpx_grid_t                                       */
+    int32_t precision;    /* hpx_precision_t                                  */
+    int32_t batch_chunk;  /* maps per internal pass (0 = default 64)          */
+    int32_t device;
+    int32_t flags;        /* HPX_FLAG_* bits                                  */
+    int32_t reserved;     /* must be 0                                        */
+} hpx_latlon_desc_t;
+HPX_API int hpx_plan_create_latlon(const hpx_latlon_desc_t* desc, hpx_plan_t* plan);
+
 /* Bytes of the plan's resident Legendre table (0 when it has none). */
 HPX_API int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes);
 

@@ -294,3 +294,21 @@ def test_refined_gradient_fd(hpx, cuda):
         fd = ((sht(f + eps * v).abs() ** 2).sum() - (sht(f - eps * v).abs() ** 2).sum()) / (2 * eps)
     an = torch.sum(f.grad * v)
     assert abs(fd.item() - an.item()) <= 1e-6 * abs(an.item())
+
+
+def test_conjugated_inputs_and_cotangents(cuda):
+    """Lazily conjugated tensors (from .conj()) are accepted as coefficients and
+    as incoming gradients."""
+    import cuhpx_b200 as hpx
+
+    rng = np.random.default_rng(21)
+    nside, L = 8, 17
+    f = torch.from_numpy(rng.standard_normal((2, 12 * nside * nside))).to(cuda).requires_grad_(True)
+    c = torch.from_numpy(rng.standard_normal((2, L, L)) + 1j * rng.standard_normal((2, L, L))).to(cuda)
+    a = hpx.SHTCUDA(nside, lmax=L, mmax=L)(f)
+    loss = (a.conj() * c).real.sum()
+    loss.backward()
+    assert abs(loss.item() - float((f.detach() * f.grad).sum())) < 1e-10 * max(1.0, abs(loss.item()))
+    g = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(a.detach().conj())
+    g2 = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(a.detach().conj().resolve_conj())
+    assert torch.equal(g, g2)
