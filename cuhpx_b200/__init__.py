@@ -9,6 +9,7 @@ from . import sht_tools
 from .hpx_sht import (LatLonPlan, Plan, SHTCUDA, SHTFunction, clear_plan_cache, get_latlon_plan, get_plan, iSHTCUDA,
                       iSHTFunction)
 from .latlon import InverseRealSHT, RealSHT
+from .ragged import RaggedISHT, RaggedSHT, split_by_offsets
 from .regrid import Grid, Regridding
 
 __all__ = [
@@ -23,6 +24,9 @@ __all__ = [
     "InverseRealSHT",
     "Grid",
     "Regridding",
+    "RaggedSHT",
+    "RaggedISHT",
+    "split_by_offsets",
     "get_plan",
     "clear_plan_cache",
     "sht_tools",

@@ -1168,6 +1168,47 @@ int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
     return HPX_OK;
 }
 
+int hpx_ragged_workspace_size(const hpx_plan_t* plans, int32_t n_groups, const int64_t* batches, size_t* bytes) {
+    if (!plans || !batches || !bytes || n_groups < 0) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    size_t need = 0;
+    for (int g = 0; g < n_groups; ++g) {
+        if (!plans[g] || batches[g] < 0) return set_err(HPX_ERR_INVALID_ARG, "invalid group " + std::to_string(g));
+        size_t b = 0;
+        hpx_workspace_size(plans[g], batches[g], &b);
+        need = std::max(need, b);
+    }
+    *bytes = need;
+    return HPX_OK;
+}
+
+namespace {
+int ragged(Op op, const hpx_plan_t* plans, int32_t n_groups, const void* const* ins, void* const* outs,
+           const int64_t* batches, void* ws, size_t ws_bytes, void* stream) {
+    if (!plans || !ins || !outs || !batches || n_groups < 0) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    for (int g = 0; g < n_groups; ++g) {
+        if (!plans[g] || batches[g] < 0 || (batches[g] > 0 && (!ins[g] || !outs[g])))
+            return set_err(HPX_ERR_INVALID_ARG, "invalid group " + std::to_string(g));
+        if (plans[g]->device != plans[0]->device) return set_err(HPX_ERR_INVALID_ARG, "plans on different devices");
+        const int rc = check_call(plans[g], ins[g], outs[g], batches[g], ws, ws_bytes);
+        if (rc != HPX_OK) return rc;
+    }
+    for (int g = 0; g < n_groups; ++g) {
+        const int rc = dispatch(plans[g], op, ins[g], outs[g], batches[g], ws, ws_bytes, stream);
+        if (rc != HPX_OK) return rc;
+    }
+    return HPX_OK;
+}
+}  // namespace
+
+int hpx_ragged_forward(const hpx_plan_t* plans, int32_t n_groups, const void* const* maps, void* const* alms,
+                       const int64_t* batches, void* ws, size_t ws_bytes, void* stream) {
+    return ragged(kForward, plans, n_groups, maps, alms, batches, ws, ws_bytes, stream);
+}
+int hpx_ragged_inverse(const hpx_plan_t* plans, int32_t n_groups, const void* const* alms, void* const* maps,
+                       const int64_t* batches, void* ws, size_t ws_bytes, void* stream) {
+    return ragged(kInverse, plans, n_groups, alms, maps, batches, ws, ws_bytes, stream);
+}
+
 int hpx_sht_forward(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* ws, size_t ws_bytes,
                     void* stream) {
     return dispatch(plan, kForward, map, alm, batch, ws, ws_bytes, stream);

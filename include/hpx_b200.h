@@ -136,6 +136,23 @@ HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void*
  * device current); make that first call before any stream capture. */
 HPX_API int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream);
 
+/* Ragged batches: n_groups groups of maps, group g with its own plan (for
+ * instance one plan per nside) transforming batches[g] contiguous maps
+ * ins[g] -> outs[g], all in one call on one stream with one workspace of
+ * hpx_ragged_workspace_size bytes (the groups run one after another and
+ * reuse it).  Replaces a per-map loop over SHTCUDA objects; the sequence of
+ * launches can be captured once in a CUDA graph.  An invalid group (null
+ * plan or pointer, negative batch) fails the call before anything runs.
+ * The plans must live on one device. */
+HPX_API int hpx_ragged_workspace_size(const hpx_plan_t* plans, int32_t n_groups, const int64_t* batches,
+                                      size_t* bytes);
+HPX_API int hpx_ragged_forward(const hpx_plan_t* plans, int32_t n_groups, const void* const* maps,
+                               void* const* alms, const int64_t* batches, void* workspace, size_t workspace_bytes,
+                               void* stream);
+HPX_API int hpx_ragged_inverse(const hpx_plan_t* plans, int32_t n_groups, const void* const* alms,
+                               void* const* maps, const int64_t* batches, void* workspace, size_t workspace_bytes,
+                               void* stream);
+
 /* Per-kernel timing.  While enabled, every kernel the plan launches is
  * bracketed by CUDA events recorded on the launch stream; hpx_stats_read
  * synchronises on those events and returns, per stage, the number of launches
