@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error check against the FP64 path")
+    ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged"],
+                    help="sht_isht: the headline step; ragged: 96 maps of mixed nside (analysis only)")
     ap.add_argument("--accuracy-maps", type=int, default=2)
     ap.add_argument("--cpu-sample-m", type=int, default=12)
     return ap.parse_args()
@@ -535,12 +537,78 @@ def roofline(stats, args, prec, refine, nside, L, B):
 FP32_SIMT_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
+def run_ragged(args):
+    """96 maps, nside drawn uniformly from {64, 128, 256, 512, 1024} (seed 4),
+    L = M = 2 nside - 1 each, N(0, 1) pixels: analysis of all of them per step,
+    (a) as a loop of one SHTCUDA call per map, (b) as one ragged call, (c) as
+    the replay of that call captured in a CUDA graph."""
+    import torch
+
+    import cuhpx_b200 as hpx
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    prec = "f16x3" if args.precision == "auto" else args.precision
+    rng = np.random.default_rng(4)
+    draw = rng.choice([64, 128, 256, 512, 1024], size=96)
+    nsides = sorted(set(int(n) for n in draw))
+    counts = [int((draw == n).sum()) for n in nsides]
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    maps = [torch.randn((c, 12 * n * n), generator=g, device=dev) for n, c in zip(nsides, counts)]
+    singles = {n: hpx.SHTCUDA(n, lmax=2 * n - 1, mmax=2 * n - 1, precision=prec) for n in nsides}
+    eager = hpx.RaggedSHT(nsides, precision=prec)
+    graphed = hpx.RaggedSHT(nsides, precision=prec, graph=True)
+    stream = torch.cuda.current_stream(dev)
+
+    def loop():
+        with torch.no_grad():
+            for n, x in zip(nsides, maps):
+                for i in range(x.shape[0]):
+                    singles[n](x[i:i + 1])
+
+    def one_call():
+        with torch.no_grad():
+            eager(maps)
+
+    def replay():
+        with torch.no_grad():
+            graphed(maps)
+
+    res = {}
+    for name, fn in (("loop", loop), ("ragged", one_call), ("graph", replay)):
+        ms = time_steps(torch, fn, args.steps, args.warmup, None, stream)
+        res[name] = 96 * args.steps / (ms / 1000.0)
+    line = {
+        "metric": "ragged SHT maps/s: 96 maps, nside in {64..1024}, L=M=2N-1",
+        "value": res["graph"],
+        "unit": "maps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 96 * 1000.0 / res["graph"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": f"f32 io, {prec} contraction",
+        "data": "synthetic",
+        "config": {"workload": "ragged analysis, 96 maps", "nsides": nsides, "counts": counts, "precision": prec},
+        "loop_maps_per_s": res["loop"],
+        "ragged_call_maps_per_s": res["ragged"],
+        "graph_replay_maps_per_s": res["graph"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ragged":
+        return run_ragged(args)
     return run_gpu(args)
 
 
