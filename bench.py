@@ -219,9 +219,9 @@ def time_steps(torch, fn, steps, warmup, dist, stream):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        from cuhpx_b200.replicas import max_over_ranks
+
+        ms = max_over_ranks(ms, device="cuda")
         dist.barrier()
     return ms
 
@@ -446,9 +446,9 @@ def e2e_pipelined(torch, sht, isht, f, dev, steps, warmup, dist):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        from cuhpx_b200.replicas import max_over_ranks
+
+        ms = max_over_ranks(ms, device="cuda")
         dist.barrier()
     return ms, steps
 
