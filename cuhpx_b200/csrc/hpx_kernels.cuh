@@ -10,13 +10,13 @@ namespace hpx {
 // (phase table, twiddles for P, and the padded work buffers of every FFT group:
 // groups x P <= 4096 whenever P <= 4096)
 __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
-    return 64 + (2 * (size_t)nmax + 63) / 64 + (size_t)pfft_max / 2 +
+    return 64 + (2 * (size_t)nmax + 63) / 64 + (size_t)padded_len(pfft_max / 2) +
            2 * (size_t)padded_len(pfft_max > 4096 ? pfft_max : 4096) + 16;
 }
 
 // One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
 template <typename T>
-__global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
+__global__ void __launch_bounds__(256, 2) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
                                                   T* __restrict__ F, int64_t Ftot, Geom geo,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
                                                   int logPmax, const cplx<T>* __restrict__ gtab,
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
     cplx<T>* elo = (cplx<T>*)smem_raw;
     cplx<T>* ehi = elo + 64;
     cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
-    cplx<T>* bufs = twP + (1 << rp.logP) / 2;
+    cplx<T>* bufs = twP + padded_len((1 << rp.logP) / 2);
     build_phase_tab(elo, ehi, rp.nphi);
     if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
     __syncthreads();
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_ring_fwd(const T* __restrict__ map, int
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
 // (ref != nullptr: write ref - synthesis)
 template <typename T>
-__global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map,
+__global__ void __launch_bounds__(256, 2) k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map,
                                                   int nmaps, int maps_per_cta, Geom geo,
                                                   const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
                                                   int logPmax, const cplx<T>* __restrict__ gtab,
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(256) k_ring_inv(const T* __restrict__ F, int64
     cplx<T>* elo = (cplx<T>*)smem_raw;
     cplx<T>* ehi = elo + 64;
     cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
-    cplx<T>* bufs = twP + (1 << rp.logP) / 2;
+    cplx<T>* bufs = twP + padded_len((1 << rp.logP) / 2);
     build_phase_tab(elo, ehi, rp.nphi);
     if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
     __syncthreads();

@@ -214,7 +214,7 @@ int create_typed(hpx_plan_s* P) {
         k_twiddles<double><<<(Pmax / 2 + 255) / 256, 256>>>(tw64, Pmax);
         HPX_CUDA_TRY(cudaMalloc(&P->d_gtab, (size_t)gsize * sizeof(C)));
         HPX_CUDA_TRY(cudaMalloc(&P->d_chirp, (size_t)gsize * sizeof(C)));
-        size_t sm = (size_t)(2 * padded_len(Pmax) + Pmax / 2) * sizeof(cplx<double>);
+        size_t sm = (size_t)(2 * padded_len(Pmax) + padded_len(Pmax / 2)) * sizeof(cplx<double>);
         int dmax = 0;
         HPX_CUDA_TRY(cudaDeviceGetAttribute(&dmax, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
         if ((int)sm > dmax) return set_err(HPX_ERR_UNSUPPORTED, "nside too large for the chirp precompute");

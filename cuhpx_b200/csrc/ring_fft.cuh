@@ -154,18 +154,42 @@ __device__ __forceinline__ void dftR(cplx<T>* v) {
     }
 }
 
+// W^r for r = 1 .. R-1 from W (one table load per butterfly): W^2, W^4, W^8 by
+// squaring, every other power as the product of two of these or of W, so each
+// carries at most a few roundings.
+template <typename T, int R>
+__device__ __forceinline__ void twiddle_powers(cplx<T> w1, cplx<T>* w) {
+    w[1] = w1;
+    if constexpr (R > 2) {
+        w[2] = cmul(w1, w1);
+        w[3] = cmul(w[2], w1);
+    }
+    if constexpr (R > 4) {
+        w[4] = cmul(w[2], w[2]);
+        w[5] = cmul(w[4], w1);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+    if constexpr (R > 8) {
+        w[8] = cmul(w[4], w[4]);
+#pragma unroll
+        for (int r = 9; r < 16; ++r) w[r] = cmul(w[8], w[r - 8]);
+    }
+}
+
 // One Stockham pass of radix R over a length-P sequence whose first Ns-point
 // sub-transforms are done: inputs src[j + rQ] (Q = P/R), outputs dst[o + r Ns]
-// with o = (j mod Ns) + R (j - j mod Ns).  Twiddles e^{-/+2 pi i r k/(Ns R)}
-// are read from twP (q < P/2) with e^{-2 pi i (q + P/2)/P} = -twP[q], never
-// built by repeated multiplication.  The first pass maps its inputs through
-// pre(i, v) (natural index i), the last pass its outputs through post(i, v).
+// with o = (j mod Ns) + R (j - j mod Ns).  Twiddles e^{-/+2 pi i r k/(Ns R)}:
+// one load of e^{-2 pi i k step/P} (step = P/(Ns R); k step < P/16) from the
+// padded table twP[padi(q)] -- the padding keeps the strided indices k step of
+// a warp on distinct banks -- and its powers by twiddle_powers.  The first pass
+// maps its inputs through pre(i, v) (natural index i), the last pass its
+// outputs through post(i, v).
 template <typename T, bool INV, int R, bool FIRST, bool LAST, typename Pre, typename Post>
 __device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P, int Ns,
                                          const cplx<T>* __restrict__ twP, int lt, int tpf, Pre& pre, Post& post) {
     const int Q = P / R;
     const int step = P / (Ns * R);
-    const int half = P >> 1;
     for (int j = lt; j < Q; j += tpf) {
         const int k = j & (Ns - 1);
         cplx<T> v[R];
@@ -175,13 +199,12 @@ __device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
         if (Ns > 1) {
+            cplx<T> w1 = twP[padi(k * step)];
+            if (INV) w1.im = -w1.im;
+            cplx<T> w[R];
+            twiddle_powers<T, R>(w1, w);
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                const int q = r * k * step;
-                cplx<T> w = q < half ? twP[q] : cplx<T>{-twP[q - half].re, -twP[q - half].im};
-                if (INV) w.im = -w.im;
-                v[r] = cmul(v[r], w);
-            }
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
         }
         dftR<T, INV, R>(v);
         const int o = ((j - k) * R) + k;
@@ -202,7 +225,7 @@ struct IdentityMap {
 // Stockham autosort FFT of length P = 2^logP (logP >= 1) on src (natural
 // order, padded indexing); returns the buffer (src or dst) holding the
 // natural-order result.  One radix-2/4/8 pass for logP mod 4, then radix-16
-// passes: 3 passes for P = 4096.  twP[q] = e^{-2 pi i q/P}, q < P/2 (shared).
+// passes: 3 passes for P = 4096.  twP: padded twiddle table (load_twiddles).
 // INV: e^{+2 pi i jk/P} (unnormalised).  pre/post as in fft_pass.
 template <typename T, bool INV, typename Pre, typename Post>
 __device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
@@ -245,12 +268,119 @@ __device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>
     return src;
 }
 
-// twP[q] = e^{-2 pi i q / P}, q < P/2, from the plan's table for Pmax (all threads of the CTA)
+// ---------------------------------------------------------------- size-specialised FFT
+// The ring kernels run one group of fft_tpf(P) threads per transform, so for
+// every length the whole pass sequence can be instantiated with P, the pass
+// strides and the group size as compile-time constants: the padded indices
+// and twiddle indices then fold into immediate offsets and shifts instead of
+// the integer arithmetic of the generic passes.
+HPX_HD constexpr int fft_tpf(int P) { return P / 16 < 32 ? 32 : (P / 16 > 256 ? 256 : P / 16); }
+HPX_HD constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
+
+// padded index of i + r * S when the stride S is a multiple of 16 (then the
+// padding of i + rS is the padding of i plus r S/16)
+template <int S>
+__device__ __forceinline__ int padi_step(int pi, int i, int r) {
+    if constexpr (S % 16 == 0) return pi + r * (S + S / 16);
+    else return padi(i + r * S);
+}
+
+template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, typename Pre, typename Post>
+__device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
+                                            Pre& pre, Post& post) {
+    constexpr int Q = P / R;
+    constexpr int LSTEP = ilog2c(P / (NS * R));
+#pragma unroll
+    for (int j0 = 0; j0 < Q; j0 += TPF) {
+        const int j = j0 + lt;
+        if (Q % TPF != 0 && j >= Q) break;
+        const int k = j & (NS - 1);
+        const int pj = padi(j);
+        cplx<T> v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            v[r] = src[padi_step<Q>(pj, j, r)];
+            if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
+        }
+        if constexpr (NS > 1) {
+            cplx<T> w1 = twP[padi(k << LSTEP)];
+            if (INV) w1.im = -w1.im;
+            cplx<T> w[R];
+            twiddle_powers<T, R>(w1, w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+        }
+        dftR<T, INV, R>(v);
+        const int o = ((j - k) * R) + k;
+        const int po = padi(o);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            cplx<T> x = v[r];
+            if constexpr (LAST) x = post(o + r * NS, x);
+            dst[padi_step<NS>(po, o, r)] = x;
+        }
+    }
+}
+
+// radix-16 passes NS, 16 NS, ... until the length is P
+template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, typename Pre, typename Post>
+__device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
+                                               int g, Pre& pre, Post& post) {
+    if constexpr (NS >= P) {
+        return src;
+    } else {
+        constexpr bool LAST = NS * 16 == P;
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST>(src, dst, twP, lt, pre, post);
+        group_sync(TPF, g);
+        return fft_r16_ct<T, INV, P, TPF, NS * 16, false>(dst, src, twP, lt, g, pre, post);
+    }
+}
+
+template <typename T, bool INV, int LOGP, typename Pre, typename Post>
+__device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
+                                           int g, Pre& pre, Post& post) {
+    constexpr int P = 1 << LOGP, TPF = fft_tpf(P), R0 = 1 << (LOGP & 3);
+    if constexpr (R0 > 1) {
+        constexpr bool LAST = R0 == P;
+        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST>(src, dst, twP, lt, pre, post);
+        group_sync(TPF, g);
+        return fft_r16_ct<T, INV, P, TPF, R0, false>(dst, src, twP, lt, g, pre, post);
+    } else {
+        return fft_r16_ct<T, INV, P, TPF, 1, true>(src, dst, twP, lt, g, pre, post);
+    }
+}
+
+// The ring kernels' FFT: the specialised pass sequence for the group size
+// fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).
+template <typename T, bool INV, typename Pre, typename Post>
+__device__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
+                             int g, Pre pre, Post post) {
+    if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
+    switch (logP) {
+        case 1: return fft_ct<T, INV, 1>(src, dst, twP, lt, g, pre, post);
+        case 2: return fft_ct<T, INV, 2>(src, dst, twP, lt, g, pre, post);
+        case 3: return fft_ct<T, INV, 3>(src, dst, twP, lt, g, pre, post);
+        case 4: return fft_ct<T, INV, 4>(src, dst, twP, lt, g, pre, post);
+        case 5: return fft_ct<T, INV, 5>(src, dst, twP, lt, g, pre, post);
+        case 6: return fft_ct<T, INV, 6>(src, dst, twP, lt, g, pre, post);
+        case 7: return fft_ct<T, INV, 7>(src, dst, twP, lt, g, pre, post);
+        case 8: return fft_ct<T, INV, 8>(src, dst, twP, lt, g, pre, post);
+        case 9: return fft_ct<T, INV, 9>(src, dst, twP, lt, g, pre, post);
+        case 10: return fft_ct<T, INV, 10>(src, dst, twP, lt, g, pre, post);
+        case 11: return fft_ct<T, INV, 11>(src, dst, twP, lt, g, pre, post);
+        case 12: return fft_ct<T, INV, 12>(src, dst, twP, lt, g, pre, post);
+        case 13: return fft_ct<T, INV, 13>(src, dst, twP, lt, g, pre, post);
+        default: return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
+    }
+}
+
+// twP[padi(q)] = e^{-2 pi i q / P}, q < P/2, from the plan's table for Pmax
+// (all threads of the CTA); the table takes padded_len(P/2) entries
 template <typename T>
 __device__ void load_twiddles(cplx<T>* twP, int logP, const cplx<T>* __restrict__ tw, int logPmax) {
     const int half = 1 << (logP - 1);
     const int stride = 1 << (logPmax - logP);
-    for (int q = threadIdx.x; q < half; q += blockDim.x) twP[q] = tw[q * stride];
+    for (int q = threadIdx.x; q < half; q += blockDim.x) twP[padi(q)] = tw[q * stride];
 }
 
 // e^{-i pi q / n} for 0 <= q < 2n from two small tables: q = 64*hi + lo
@@ -283,8 +413,8 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
     IdentityMap id;
     if (rp.logh >= 0) {
         if (rp.logh == 0) return buf;
-        return inv ? fft_pow2<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id)
-                   : fft_pow2<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id);
+        return inv ? fft_ring<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id)
+                   : fft_ring<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id);
     }
     // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
     // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
@@ -304,9 +434,9 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         if (inv) v.im = -v.im;
         return v;
     };
-    cplx<T>* r = fft_pow2<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
+    cplx<T>* r = fft_ring<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
     cplx<T>* o = (r == buf) ? buf2 : buf;
-    return fft_pow2<T, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
+    return fft_ring<T, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
 }
 
 // Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
