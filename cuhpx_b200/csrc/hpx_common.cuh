@@ -119,4 +119,19 @@ HPX_HD cplx<T> cconj(cplx<T> a) { return {a.re, -a.im}; }
 template <typename T>
 HPX_HD cplx<T> cscale(cplx<T> a, T s) { return {a.re * s, a.im * s}; }
 
+// ------------------------------------------------------------------ async copies
+// cp.async global -> shared: 16 bytes (zero fill when !valid), or 8 bytes
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid = true) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 }  // namespace hpx

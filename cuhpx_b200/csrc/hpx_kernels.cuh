@@ -46,9 +46,15 @@ __global__ void __launch_bounds__(256, 2) k_ring_fwd(const T* __restrict__ map, 
     const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
+    cplx<T>* cur = buf;
+    cplx<T>* other = buf2;
+    if (b0 + g < b1) ring_load_async(cur, map + (int64_t)(b0 + g) * np + start, rp.h, lt, tpf);
     for (int b = b0 + g; b < b1; b += S) {
-        const T mx = ring_forward(map + (int64_t)b * np + start, shift, buf, buf2, F + 2 * ((int64_t)b * Ftot + foff),
-                                  rp, twP, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+        auto load_next = [&](cplx<T>* dst) {
+            if (b + S < b1) ring_load_async(dst, map + (int64_t)(b + S) * np + start, rp.h, lt, tpf);
+        };
+        const T mx = ring_forward(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, twP, gtab,
+                                  chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
         if (fmax) {
             // per-map max |F| (scale of the FP16 operands); a group is whole warps
             float v = (float)mx;
@@ -91,10 +97,17 @@ __global__ void __launch_bounds__(256, 2) k_ring_inv(const T* __restrict__ F, in
     const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
-    for (int b = b0 + g; b < b1; b += S)
-        ring_inverse((const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + foff)), shift, buf, buf2,
-                     map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr, rp, twP, gtab,
-                     chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g);
+    cplx<T>* cur = buf;
+    cplx<T>* other = buf2;
+    auto spec = [&](int bb) { return (const cplx<T>*)(F + 2 * ((int64_t)bb * Ftot + foff)); };
+    if (b0 + g < b1) spec_load_async(cur, spec(b0 + g), rp.mt, lt, tpf);
+    for (int b = b0 + g; b < b1; b += S) {
+        auto load_next = [&](cplx<T>* dst) {
+            if (b + S < b1) spec_load_async(dst, spec(b + S), rp.mt, lt, tpf);
+        };
+        ring_inverse(cur, other, shift, map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr,
+                     rp, twP, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
+    }
 }
 
 // Per-map max |x| over rows of n floats: atomicMax of the float bits into out[map]

@@ -203,14 +203,6 @@ __host__ __device__ constexpr size_t fwd_smem_bytes() {
            (size_t)2 * C::KC * 2 * C::CT * sizeof(T) + 64;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec, int C, int nmaps,

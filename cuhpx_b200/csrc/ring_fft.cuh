@@ -439,17 +439,44 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
     return fft_ring<T, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
 }
 
-// Forward transform of one real ring x[0..n) into F[0..mt) (global, contiguous).
-// Returns the largest |re|, |im| this thread wrote.
+// One complex element (8 or 16 bytes) global -> shared, asynchronously.
 template <typename T>
-__device__ T ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ F,
-                             const RingPair& rp, const cplx<T>* __restrict__ twP, const cplx<T>* __restrict__ gtab,
-                             const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g) {
+__device__ __forceinline__ void cp_async_cplx(cplx<T>* dst, const cplx<T>* src) {
+    if constexpr (sizeof(T) == 4) cp_async8(dst, src);
+    else cp_async16(dst, src);
+}
+
+// The group starts copying ring x[0..n) (h complex) into dst[padi(j)]; the copy
+// is one cp.async commit group of the calling threads.
+template <typename T>
+__device__ __forceinline__ void ring_load_async(cplx<T>* dst, const T* x, int h, int lt, int tpf) {
+    for (int j = lt; j < h; j += tpf) cp_async_cplx(dst + padi(j), (const cplx<T>*)x + j);
+    cp_async_commit();
+}
+
+// ... and the spectrum Fg[0..mt) into dst[0..mt) (contiguous).
+template <typename T>
+__device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg, int mt, int lt, int tpf) {
+    for (int k = lt; k < mt; k += tpf) cp_async_cplx(dst + k, Fg + k);
+    cp_async_commit();
+}
+
+// Forward transform of one real ring into F[0..mt) (global, contiguous).  The
+// ring was loaded into cur[padi(j)] by ring_load_async; the two FFT buffers
+// alternate roles from map to map: once the DFT is done, the buffer it left
+// free receives the next map's ring (load_next, asynchronous) while this map's
+// spectrum is formed and stored.  On return cur holds the next input.
+// Returns the largest |re|, |im| this thread wrote.
+template <typename T, typename Next>
+__device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ F, const RingPair& rp,
+                          const cplx<T>* __restrict__ twP, const cplx<T>* __restrict__ gtab,
+                          const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g,
+                          Next load_next) {
     const int h = rp.h;
-    for (int j = lt; j < h; j += tpf) {
-        buf[padi(j)] = *(const cplx<T>*)(x + 2 * j);
-    }
-    cplx<T>* Z = ring_dft(buf, buf2, rp, twP, gtab, chirp, false, lt, tpf, g);
+    cp_async_wait<0>();
+    cplx<T>* Z = ring_dft(cur, other, rp, twP, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
+    cplx<T>* freeb = (Z == cur) ? other : cur;
+    load_next(freeb);
     T mx = (T)0;
     for (int k = lt; k < rp.mt; k += tpf) {
         const int k1 = k == h ? 0 : k;
@@ -465,22 +492,27 @@ __device__ T ring_forward(const T* __restrict__ x, int shift, cplx<T>* buf, cplx
         mx = fmax(mx, fmax(fabs(X.re), fabs(X.im)));
     }
     group_sync(tpf, g);
+    cur = freeb;
+    other = Z;
     return mx;
 }
 
-// Inverse transform of the ring spectrum Fg[0..mt) (global) into one real ring
-// x[0..n).  The spectrum is staged once, contiguously, into buf2 (free until
-// the DFT starts), because each output needs both F[k] and F[h-k].
-// ref != nullptr: write ref - x (Jacobi residual).
-template <typename T>
-__device__ void ring_inverse(const cplx<T>* __restrict__ Fg, int shift, cplx<T>* buf, cplx<T>* buf2, T* __restrict__ x,
+// Inverse transform of one ring spectrum into the real ring x[0..n).  The
+// spectrum Fg[0..mt) was loaded into cur[0..mt) by spec_load_async (each
+// output needs both F[k] and F[h-k]); it is unpacked into other[padi(k)], the
+// DFT runs there, and the buffer it leaves free receives the next map's
+// spectrum (load_next) while this ring is stored.  On return cur holds the
+// next input.  ref != nullptr: write ref - x (Jacobi residual).
+template <typename T, typename Next>
+__device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ x,
                              const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ twP,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
-                             const PhaseTab<T>& E, int lt, int tpf, int g) {
+                             const PhaseTab<T>& E, int lt, int tpf, int g, Next load_next) {
     const int h = rp.h, mt = rp.mt;
-    for (int k = lt; k < mt; k += tpf) buf2[k] = Fg[k];
+    cp_async_wait<0>();
     group_sync(tpf, g);
-    const cplx<T>* Fs = buf2;
+    const cplx<T>* Fs = cur;
+    cplx<T>* buf = other;
     for (int k = lt; k < h; k += tpf) {
         // X_k and conj(X_{h-k}) with the phase e^{+i s k pi/n}; imag of X_0, X_h dropped
         cplx<T> Xa = {(T)0, (T)0}, Xb = {(T)0, (T)0};
@@ -495,7 +527,9 @@ __device__ void ring_inverse(const cplx<T>* __restrict__ Fg, int shift, cplx<T>*
         const cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
         buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
     }
-    cplx<T>* z = ring_dft(buf, buf2, rp, twP, gtab, chirp, true, lt, tpf, g);
+    cplx<T>* z = ring_dft(buf, cur, rp, twP, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
+    cplx<T>* freeb = (z == buf) ? cur : buf;
+    load_next(freeb);
     for (int j = lt; j < h; j += tpf) {
         cplx<T> v = z[padi(j)];
         if (ref) {
@@ -505,6 +539,8 @@ __device__ void ring_inverse(const cplx<T>* __restrict__ Fg, int shift, cplx<T>*
         *(cplx<T>*)(x + 2 * j) = v;
     }
     group_sync(tpf, g);
+    cur = freeb;
+    other = z;
 }
 
 }  // namespace hpx
