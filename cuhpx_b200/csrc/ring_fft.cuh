@@ -478,18 +478,32 @@ __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restri
     cplx<T>* freeb = (Z == cur) ? other : cur;
     load_next(freeb);
     T mx = (T)0;
-    for (int k = lt; k < rp.mt; k += tpf) {
-        const int k1 = k == h ? 0 : k;
-        const int k2 = k == 0 ? 0 : h - k;
-        const cplx<T> Zk = Z[padi(k1)];
-        const cplx<T> Zc = cconj(Z[padi(k2)]);
+    // Outputs k and h-k share Z_k, Z_{h-k} and the twiddle W = e^{-2 pi i k/n}:
+    // X_k = E_k + W O_k and X_{h-k} = conj(E_k - W O_k); the ring phase of h-k
+    // is e^{-i pi (h-k)/n} = -i conj(e^{-i pi k/n}).
+    const int mt = rp.mt;
+    for (int k = lt; 2 * k <= h; k += tpf) {
+        const int kb = h - k;
+        const cplx<T> Zk = Z[padi(k)];
+        const cplx<T> Zc = cconj(Z[padi(k == 0 ? 0 : kb)]);
         const cplx<T> Ek = cscale(cadd(Zk, Zc), (T)0.5);
         const cplx<T> d = cscale(csub(Zk, Zc), (T)0.5);
-        const cplx<T> Ok = {d.im, -d.re};  // -i * d
-        cplx<T> X = cadd(Ek, cmul(E(2 * k), Ok));
-        if (shift) X = cmul(E(k), X);
-        *(cplx<T>*)(F + 2 * k) = X;
-        mx = fmax(mx, fmax(fabs(X.re), fabs(X.im)));
+        const cplx<T> WO = cmul(E(2 * k), cplx<T>{d.im, -d.re});  // W (-i d)
+        cplx<T> Xa = cadd(Ek, WO);
+        cplx<T> Xb = cconj(csub(Ek, WO));
+        if (shift) {
+            const cplx<T> e = E(k);
+            Xa = cmul(e, Xa);
+            Xb = cmul(cplx<T>{-e.im, -e.re}, Xb);
+        }
+        if (k < mt) {
+            *(cplx<T>*)(F + 2 * k) = Xa;
+            mx = fmax(mx, fmax(fabs(Xa.re), fabs(Xa.im)));
+        }
+        if (kb != k && kb < mt) {
+            *(cplx<T>*)(F + 2 * kb) = Xb;
+            mx = fmax(mx, fmax(fabs(Xb.re), fabs(Xb.im)));
+        }
     }
     group_sync(tpf, g);
     cur = freeb;
@@ -513,12 +527,16 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
     group_sync(tpf, g);
     const cplx<T>* Fs = cur;
     cplx<T>* buf = other;
-    for (int k = lt; k < h; k += tpf) {
+    // Entries k and h-k share F_k, F_{h-k} and one twiddle: buf_{h-k} =
+    // conj(sum - i r) for buf_k = sum + i r, and conj of the ring phase of h-k
+    // is i e^{-i pi k/n}.
+    for (int k = lt; 2 * k <= h; k += tpf) {
         // X_k and conj(X_{h-k}) with the phase e^{+i s k pi/n}; imag of X_0, X_h dropped
-        cplx<T> Xa = {(T)0, (T)0}, Xb = {(T)0, (T)0};
-        if (k < mt) Xa = shift ? cmul(Fs[k], cconj(E(k))) : Fs[k];
         const int kb = h - k;
-        if (kb < mt) Xb = cconj(shift ? cmul(Fs[kb], cconj(E(kb))) : Fs[kb]);
+        const cplx<T> e = shift ? E(k) : cplx<T>{(T)1, (T)0};
+        cplx<T> Xa = {(T)0, (T)0}, Xb = {(T)0, (T)0};
+        if (k < mt) Xa = shift ? cmul(Fs[k], cconj(e)) : Fs[k];
+        if (kb < mt) Xb = cconj(shift ? cmul(Fs[kb], cplx<T>{-e.im, e.re}) : Fs[kb]);
         if (k == 0) {
             Xa.im = (T)0;
             Xb.im = (T)0;
@@ -526,6 +544,7 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
         const cplx<T> sum = cadd(Xa, Xb), dif = csub(Xa, Xb);
         const cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
         buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
+        if (k != 0 && kb != k) buf[padi(kb)] = {sum.re + r.im, r.re - sum.im};
     }
     cplx<T>* z = ring_dft(buf, cur, rp, twP, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
