@@ -422,13 +422,15 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
     // products ride on the first loads and the last stores of the two FFTs.
     const int h = rp.h;
     const cplx<T>* G = gtab + rp.gtab_off;
-    auto pre = [&](int j, cplx<T> a) {
+    // captures by value: the passes may run in a called (not inlined) function,
+    // where a captured reference would be a load from the stack per element
+    auto pre = [h, inv, chirp](int j, cplx<T> a) {
         if (j >= h) return cplx<T>{(T)0, (T)0};
         if (inv) a.im = -a.im;
         return cmul(a, chirp[j]);
     };
-    auto mulG = [&](int k, cplx<T> a) { return cmul(a, G[k]); };
-    auto postc = [&](int k, cplx<T> a) {
+    auto mulG = [G](int k, cplx<T> a) { return cmul(a, G[k]); };
+    auto postc = [h, inv, chirp](int k, cplx<T> a) {
         if (k >= h) return a;
         cplx<T> v = cmul(a, chirp[k]);
         if (inv) v.im = -v.im;
