@@ -285,7 +285,11 @@ __device__ __forceinline__ int padi_step(int pi, int i, int r) {
     else return padi(i + r * S);
 }
 
-template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, typename Pre, typename Post>
+// ZIN: the input is zero from P/2 on (the first pass then loads and transforms
+// only R/2 of its R inputs); HOUT: only outputs below P/2 are wanted (the last
+// pass forms and stores only those).  Bluestein's convolution has both.
+template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT,
+          typename Pre, typename Post>
 __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
                                             Pre& pre, Post& post) {
     constexpr int Q = P / R;
@@ -299,6 +303,10 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
         cplx<T> v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
+            if (FIRST && ZIN && 2 * r >= R) {
+                v[r] = {(T)0, (T)0};  // j + r Q >= P/2
+                continue;
+            }
             v[r] = src[padi_step<Q>(pj, j, r)];
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
@@ -315,6 +323,7 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
         const int po = padi(o);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
+            if (LAST && HOUT && 2 * r >= R) continue;  // o + r NS >= P/2
             cplx<T> x = v[r];
             if constexpr (LAST) x = post(o + r * NS, x);
             dst[padi_step<NS>(po, o, r)] = x;
@@ -323,53 +332,55 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
 }
 
 // radix-16 passes NS, 16 NS, ... until the length is P
-template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, typename Pre, typename Post>
+template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
                                                int g, Pre& pre, Post& post) {
     if constexpr (NS >= P) {
         return src;
     } else {
         constexpr bool LAST = NS * 16 == P;
-        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST>(src, dst, twP, lt, pre, post);
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT>(src, dst, twP, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, NS * 16, false>(dst, src, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT>(dst, src, twP, lt, g, pre, post);
     }
 }
 
-template <typename T, bool INV, int LOGP, typename Pre, typename Post>
+template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
                                            int g, Pre& pre, Post& post) {
     constexpr int P = 1 << LOGP, TPF = fft_tpf(P), R0 = 1 << (LOGP & 3);
     if constexpr (R0 > 1) {
         constexpr bool LAST = R0 == P;
-        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST>(src, dst, twP, lt, pre, post);
+        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT>(src, dst, twP, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, R0, false>(dst, src, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT>(dst, src, twP, lt, g, pre, post);
     } else {
-        return fft_r16_ct<T, INV, P, TPF, 1, true>(src, dst, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
     }
 }
 
 // The ring kernels' FFT: the specialised pass sequence for the group size
-// fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).
-template <typename T, bool INV, typename Pre, typename Post>
+// fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).  ZIN / HOUT
+// as for fft_pass_ct (the generic passes ignore them: they transform and store
+// everything, which is also correct).
+template <typename T, bool INV, bool ZIN = false, bool HOUT = false, typename Pre, typename Post>
 __device__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
                              int g, Pre pre, Post post) {
     if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
     switch (logP) {
-        case 1: return fft_ct<T, INV, 1>(src, dst, twP, lt, g, pre, post);
-        case 2: return fft_ct<T, INV, 2>(src, dst, twP, lt, g, pre, post);
-        case 3: return fft_ct<T, INV, 3>(src, dst, twP, lt, g, pre, post);
-        case 4: return fft_ct<T, INV, 4>(src, dst, twP, lt, g, pre, post);
-        case 5: return fft_ct<T, INV, 5>(src, dst, twP, lt, g, pre, post);
-        case 6: return fft_ct<T, INV, 6>(src, dst, twP, lt, g, pre, post);
-        case 7: return fft_ct<T, INV, 7>(src, dst, twP, lt, g, pre, post);
-        case 8: return fft_ct<T, INV, 8>(src, dst, twP, lt, g, pre, post);
-        case 9: return fft_ct<T, INV, 9>(src, dst, twP, lt, g, pre, post);
-        case 10: return fft_ct<T, INV, 10>(src, dst, twP, lt, g, pre, post);
-        case 11: return fft_ct<T, INV, 11>(src, dst, twP, lt, g, pre, post);
-        case 12: return fft_ct<T, INV, 12>(src, dst, twP, lt, g, pre, post);
-        case 13: return fft_ct<T, INV, 13>(src, dst, twP, lt, g, pre, post);
+        case 1: return fft_ct<T, INV, 1, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 2: return fft_ct<T, INV, 2, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 3: return fft_ct<T, INV, 3, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 4: return fft_ct<T, INV, 4, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 5: return fft_ct<T, INV, 5, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 6: return fft_ct<T, INV, 6, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 7: return fft_ct<T, INV, 7, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 8: return fft_ct<T, INV, 8, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 9: return fft_ct<T, INV, 9, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 10: return fft_ct<T, INV, 10, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 11: return fft_ct<T, INV, 11, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 12: return fft_ct<T, INV, 12, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        case 13: return fft_ct<T, INV, 13, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
         default: return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
     }
 }
@@ -436,9 +447,10 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         if (inv) v.im = -v.im;
         return v;
     };
-    cplx<T>* r = fft_ring<T, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
+    // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
+    cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
     cplx<T>* o = (r == buf) ? buf2 : buf;
-    return fft_ring<T, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
+    return fft_ring<T, true, false, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
 }
 
 // One complex element (8 or 16 bytes) global -> shared, asynchronously.
