@@ -7,34 +7,45 @@
 namespace hpx {
 
 // complex elements of dynamic shared memory the ring kernels need
-// (phase table, twiddles for P, and the padded work buffers of every FFT group:
-// groups x P <= 4096 whenever P <= 4096)
+// (the phase and twiddle tables, and the padded work buffers of every FFT
+// group: groups x P <= 4096 whenever P <= 4096)
 __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
-    return 64 + (2 * (size_t)nmax + 63) / 64 + (size_t)padded_len(pfft_max / 2) +
+    return (size_t)phase_tab_elems(nmax) + (size_t)phase_tab_elems(pfft_max / 2) +
            2 * (size_t)padded_len(pfft_max > 4096 ? pfft_max : 4096) + 16;
+}
+
+// CTAs per SM the ring kernels are compiled for: 3 x 256 threads of float
+// (80 registers; 3 x 74 KB of shared memory at P = 4096), 2 of double
+template <typename T>
+constexpr int ring_min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
+
+// shared-memory layout of a ring CTA: phase table E (e^{-i pi q/nphi}), FFT
+// twiddles (e^{-2 pi i q/P}), then the work buffers
+template <typename T>
+__device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingPair& rp, PhaseTab<T>& E,
+                                                PhaseTab<T>& tw) {
+    cplx<T>* et = (cplx<T>*)smem;
+    cplx<T>* tt = et + phase_tab_elems(rp.nphi);
+    E = build_phase_tab(et, rp.nphi);
+    const int half = (1 << rp.logP) / 2;
+    tw = rp.logP > 0 ? build_phase_tab(tt, half) : E;  // no FFT when h = 1
+    return tt + phase_tab_elems(half);
 }
 
 // One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta,
-                                                  T* __restrict__ F, int64_t Ftot, Geom geo,
-                                                  const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
-                                                  int logPmax, const cplx<T>* __restrict__ gtab,
-                                                  const cplx<T>* __restrict__ chirp,
-                                                  unsigned* __restrict__ fmax) {
+__global__ void __launch_bounds__(256, ring_min_ctas<T>())
+    k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta, T* __restrict__ F, int64_t Ftot, Geom geo,
+               const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+               unsigned* __restrict__ fmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
     const int t = blockIdx.x;
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
-    cplx<T>* elo = (cplx<T>*)smem_raw;
-    cplx<T>* ehi = elo + 64;
-    cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
-    cplx<T>* bufs = twP + padded_len((1 << rp.logP) / 2);
-    build_phase_tab(elo, ehi, rp.nphi);
-    if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
+    PhaseTab<T> E, tw;
+    cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
     __syncthreads();
-    const PhaseTab<T> E{elo, ehi};
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
     const int PL = padded_len(P);
@@ -53,7 +64,7 @@ __global__ void __launch_bounds__(256, 2) k_ring_fwd(const T* __restrict__ map, 
         auto load_next = [&](cplx<T>* dst) {
             if (b + S < b1) ring_load_async(dst, map + (int64_t)(b + S) * np + start, rp.h, lt, tpf);
         };
-        const T mx = ring_forward(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, twP, gtab,
+        const T mx = ring_forward(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, tw, gtab,
                                   chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
         if (fmax) {
             // per-map max |F| (scale of the FP16 operands); a group is whole warps
@@ -68,24 +79,18 @@ __global__ void __launch_bounds__(256, 2) k_ring_fwd(const T* __restrict__ map, 
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
 // (ref != nullptr: write ref - synthesis)
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map,
-                                                  int nmaps, int maps_per_cta, Geom geo,
-                                                  const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ tw,
-                                                  int logPmax, const cplx<T>* __restrict__ gtab,
-                                                  const cplx<T>* __restrict__ chirp, const T* __restrict__ ref) {
+__global__ void __launch_bounds__(256, ring_min_ctas<T>())
+    k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map, int nmaps, int maps_per_cta, Geom geo,
+               const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+               const T* __restrict__ ref) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
     const int t = blockIdx.x;
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
-    cplx<T>* elo = (cplx<T>*)smem_raw;
-    cplx<T>* ehi = elo + 64;
-    cplx<T>* twP = ehi + (2 * rp.nphi + 63) / 64;
-    cplx<T>* bufs = twP + padded_len((1 << rp.logP) / 2);
-    build_phase_tab(elo, ehi, rp.nphi);
-    if (rp.logP > 0) load_twiddles(twP, rp.logP, tw, logPmax);
+    PhaseTab<T> E, tw;
+    cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
     __syncthreads();
-    const PhaseTab<T> E{elo, ehi};
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
     const int PL = padded_len(P);
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(256, 2) k_ring_inv(const T* __restrict__ F, in
             if (b + S < b1) spec_load_async(dst, spec(b + S), rp.mt, lt, tpf);
         };
         ring_inverse(cur, other, shift, map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr,
-                     rp, twP, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
+                     rp, tw, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
     }
 }
 
@@ -303,8 +308,8 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
         if (j < h) chirp[rp.gtab_off + j] = {(T)v.re, (T)(-v.im)};
     }
     __syncthreads();
-    cplx<double>* r = fft_pow2<double, false>(buf, buf2, rp.logP, twP, threadIdx.x, blockDim.x, 0, IdentityMap{},
-                                              IdentityMap{});
+    cplx<double>* r = fft_pow2<double, false>(buf, buf2, rp.logP, FullTw<double>{twP}, threadIdx.x, blockDim.x, 0,
+                                              IdentityMap{}, IdentityMap{});
     const double inv = 1.0 / (double)P;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         gtab[rp.gtab_off + j] = {(T)(r[padi(j)].re * inv), (T)(r[padi(j)].im * inv)};

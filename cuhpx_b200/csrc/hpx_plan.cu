@@ -88,7 +88,6 @@ struct hpx_plan_s {
     int nmax = 0;   // max nphi
     std::vector<RingPair> h_pairs;
     RingPair* d_pairs = nullptr;
-    void* d_tw = nullptr;   // cplx<T> twiddles for the plan's FFT type
     void* d_gtab = nullptr; // cplx<T> Bluestein chirp spectra (natural order)
     void* d_chirp = nullptr; // cplx<T> Bluestein chirps
     int64_t Ftot = 0;        // complex spectrum entries per map over all rings
@@ -137,7 +136,6 @@ struct hpx_plan_s {
         cudaGetDevice(&prev);
         cudaSetDevice(device);
         cudaFree(d_pairs);
-        cudaFree(d_tw);
         cudaFree(d_gtab);
         cudaFree(d_chirp);
         cudaFree(d_lstart);
@@ -201,9 +199,6 @@ template <typename T>
 int create_typed(hpx_plan_s* P) {
     using C = cplx<T>;
     const int Pmax = 1 << P->logPmax;
-    HPX_CUDA_TRY(cudaMalloc(&P->d_tw, (size_t)(Pmax / 2) * sizeof(C)));
-    k_twiddles<T><<<(Pmax / 2 + 255) / 256, 256>>>((C*)P->d_tw, Pmax);
-    HPX_CUDA_TRY(cudaGetLastError());
     // chirp spectra computed in FP64 with FP64 twiddles
     int64_t gsize = 0;
     for (auto& rp : P->h_pairs)
@@ -803,7 +798,6 @@ struct Pipeline {
             if (fmax) cudaMemsetAsync(fmax, 0, sizeof(unsigned) * nb, st);
             dim3 grid(P->R, (nb + g - 1) / g);
             k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->geo, P->d_pairs,
-                                                          (const cplx<T>*)P->d_tw, P->logPmax,
                                                           (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, fmax);
         }
         Timer tm(P, st, kStFold);
@@ -824,8 +818,7 @@ struct Pipeline {
         Timer tm(P, st, kStRingInv);
         dim3 grid(P->R, (nb + g - 1) / g);
         k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(F, P->Ftot, map, nb, g, P->geo, P->d_pairs,
-                                                      (const cplx<T>*)P->d_tw, P->logPmax, (const cplx<T>*)P->d_gtab,
-                                                      (const cplx<T>*)P->d_chirp, ref);
+                                                      (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, ref);
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();

@@ -177,17 +177,65 @@ __device__ __forceinline__ void twiddle_powers(cplx<T> w1, cplx<T>* w) {
     }
 }
 
+// e^{-i pi q / n} for 0 <= q < 2n from small tables, q = 64 a + b:
+// e^{-i pi 64 a/n} = hi[a] + hc[a] (float + float: hc is the rounding error of
+// hi) and lo[b] = e^{-i pi b/n} - 1 (|lo| < 0.1 for n >= 2048), so that
+// hi + (hc + hi lo) rounds once, at the end, like a correctly rounded table
+// entry.  That matters for FFT twiddles, whose powers W^r multiply the error of
+// W by r.  The ring kernels keep two: the phases of the real-FFT split and
+// ring shift (n = nphi) and the FFT twiddles e^{-2 pi i q/P} (n = P/2), about
+// 1.5 KB instead of a P/2-entry twiddle table.
+template <typename T>
+struct PhaseTab {
+    const cplx<T>* lo;  // 64 entries
+    const cplx<T>* hi;  // phase_tab_nhi(n) entries, followed by as many hc entries
+    int nhi;
+    __device__ __forceinline__ cplx<T> operator()(int q) const {
+        const cplx<T> a = hi[q >> 6], c = hi[nhi + (q >> 6)], d = lo[q & 63];
+        return {a.re + fma(a.re, d.re, fma(-a.im, d.im, c.re)), a.im + fma(a.re, d.im, fma(a.im, d.re, c.im))};
+    }
+};
+
+HPX_HD constexpr int phase_tab_nhi(int n) { return (2 * n + 63) / 64; }
+// complex entries of the tables for n
+HPX_HD constexpr int phase_tab_elems(int n) { return 64 + 2 * phase_tab_nhi(n); }
+
+template <typename T>
+__device__ PhaseTab<T> build_phase_tab(cplx<T>* lo, int n) {
+    const int nhi = phase_tab_nhi(n);
+    cplx<T>* hi = lo + 64;
+    for (int i = threadIdx.x; i < 64 + nhi; i += blockDim.x) {
+        const int q = i < 64 ? i : 64 * (i - 64);
+        double s, c;
+        sincospi(-(double)q / (double)n, &s, &c);
+        if (i < 64) {
+            const double sh = sinpi((double)q / (double)(2 * n));
+            lo[i] = {(T)(-2.0 * sh * sh), (T)s};  // cos - 1 = -2 sin^2(theta/2)
+        } else {
+            const cplx<T> v = {(T)c, (T)s};
+            hi[i - 64] = v;
+            hi[nhi + i - 64] = {(T)(c - (double)v.re), (T)(s - (double)v.im)};
+        }
+    }
+    return PhaseTab<T>{lo, hi, nhi};
+}
+
+// twiddles e^{-2 pi i q/P} read from a full padded table tw[padi(q)], q < P/2
+template <typename T>
+struct FullTw {
+    const cplx<T>* p;
+    __device__ __forceinline__ cplx<T> operator()(int q) const { return p[padi(q)]; }
+};
+
 // One Stockham pass of radix R over a length-P sequence whose first Ns-point
 // sub-transforms are done: inputs src[j + rQ] (Q = P/R), outputs dst[o + r Ns]
 // with o = (j mod Ns) + R (j - j mod Ns).  Twiddles e^{-/+2 pi i r k/(Ns R)}:
-// one load of e^{-2 pi i k step/P} (step = P/(Ns R); k step < P/16) from the
-// padded table twP[padi(q)] -- the padding keeps the strided indices k step of
-// a warp on distinct banks -- and its powers by twiddle_powers.  The first pass
-// maps its inputs through pre(i, v) (natural index i), the last pass its
-// outputs through post(i, v).
-template <typename T, bool INV, int R, bool FIRST, bool LAST, typename Pre, typename Post>
-__device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P, int Ns,
-                                         const cplx<T>* __restrict__ twP, int lt, int tpf, Pre& pre, Post& post) {
+// one lookup tw(k step) = e^{-2 pi i k step/P} (step = P/(Ns R)) and its powers
+// by twiddle_powers.  The first pass maps its inputs through pre(i, v)
+// (natural index i), the last pass its outputs through post(i, v).
+template <typename T, bool INV, int R, bool FIRST, bool LAST, typename TW, typename Pre, typename Post>
+__device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P, int Ns, const TW& tw, int lt,
+                                         int tpf, Pre& pre, Post& post) {
     const int Q = P / R;
     const int step = P / (Ns * R);
     for (int j = lt; j < Q; j += tpf) {
@@ -199,7 +247,7 @@ __device__ __forceinline__ void fft_pass(const cplx<T>* src, cplx<T>* dst, int P
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
         if (Ns > 1) {
-            cplx<T> w1 = twP[padi(k * step)];
+            cplx<T> w1 = tw(k * step);
             if (INV) w1.im = -w1.im;
             cplx<T> w[R];
             twiddle_powers<T, R>(w1, w);
@@ -225,11 +273,11 @@ struct IdentityMap {
 // Stockham autosort FFT of length P = 2^logP (logP >= 1) on src (natural
 // order, padded indexing); returns the buffer (src or dst) holding the
 // natural-order result.  One radix-2/4/8 pass for logP mod 4, then radix-16
-// passes: 3 passes for P = 4096.  twP: padded twiddle table (load_twiddles).
+// passes: 3 passes for P = 4096.  tw(q) = e^{-2 pi i q/P}, q < P/2.
 // INV: e^{+2 pi i jk/P} (unnormalised).  pre/post as in fft_pass.
-template <typename T, bool INV, typename Pre, typename Post>
-__device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
-                             int g, Pre pre, Post post) {
+template <typename T, bool INV, typename TW, typename Pre, typename Post>
+__device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const TW& tw, int lt, int tpf, int g, Pre pre,
+                             Post post) {
     const int P = 1 << logP;
     const int n16 = logP >> 2, r0 = logP & 3;
     const int npass = n16 + (r0 ? 1 : 0);
@@ -244,24 +292,24 @@ __device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>
     if (r0) {
         const bool last = npass == 1;
         if (r0 == 1) {
-            if (last) fft_pass<T, INV, 2, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-            else fft_pass<T, INV, 2, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            if (last) fft_pass<T, INV, 2, true, true>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+            else fft_pass<T, INV, 2, true, false>(src, dst, P, Ns, tw, lt, tpf, pre, post);
         } else if (r0 == 2) {
-            if (last) fft_pass<T, INV, 4, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-            else fft_pass<T, INV, 4, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            if (last) fft_pass<T, INV, 4, true, true>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+            else fft_pass<T, INV, 4, true, false>(src, dst, P, Ns, tw, lt, tpf, pre, post);
         } else {
-            if (last) fft_pass<T, INV, 8, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-            else fft_pass<T, INV, 8, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+            if (last) fft_pass<T, INV, 8, true, true>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+            else fft_pass<T, INV, 8, true, false>(src, dst, P, Ns, tw, lt, tpf, pre, post);
         }
         Ns <<= r0;
         next();
     }
     for (int i = 0; i < n16; ++i) {
         const bool first = pass == 0, last = pass == npass - 1;
-        if (first && last) fft_pass<T, INV, 16, true, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-        else if (first) fft_pass<T, INV, 16, true, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-        else if (last) fft_pass<T, INV, 16, false, true>(src, dst, P, Ns, twP, lt, tpf, pre, post);
-        else fft_pass<T, INV, 16, false, false>(src, dst, P, Ns, twP, lt, tpf, pre, post);
+        if (first && last) fft_pass<T, INV, 16, true, true>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+        else if (first) fft_pass<T, INV, 16, true, false>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+        else if (last) fft_pass<T, INV, 16, false, true>(src, dst, P, Ns, tw, lt, tpf, pre, post);
+        else fft_pass<T, INV, 16, false, false>(src, dst, P, Ns, tw, lt, tpf, pre, post);
         Ns <<= 4;
         next();
     }
@@ -289,9 +337,9 @@ __device__ __forceinline__ int padi_step(int pi, int i, int r) {
 // only R/2 of its R inputs); HOUT: only outputs below P/2 are wanted (the last
 // pass forms and stores only those).  Bluestein's convolution has both.
 template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT,
-          typename Pre, typename Post>
-__device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
-                                            Pre& pre, Post& post) {
+          typename TW, typename Pre, typename Post>
+__device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, Pre& pre,
+                                            Post& post) {
     constexpr int Q = P / R;
     constexpr int LSTEP = ilog2c(P / (NS * R));
 #pragma unroll
@@ -311,7 +359,7 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
         if constexpr (NS > 1) {
-            cplx<T> w1 = twP[padi(k << LSTEP)];
+            cplx<T> w1 = tw(k << LSTEP);
             if (INV) w1.im = -w1.im;
             cplx<T> w[R];
             twiddle_powers<T, R>(w1, w);
@@ -332,30 +380,31 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
 }
 
 // radix-16 passes NS, 16 NS, ... until the length is P
-template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, typename Pre, typename Post>
-__device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
-                                               int g, Pre& pre, Post& post) {
+template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, typename TW, typename Pre,
+          typename Post>
+__device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
+                                               Post& post) {
     if constexpr (NS >= P) {
         return src;
     } else {
         constexpr bool LAST = NS * 16 == P;
-        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT>(src, dst, twP, lt, pre, post);
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT>(dst, src, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT>(dst, src, tw, lt, g, pre, post);
     }
 }
 
-template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, typename Pre, typename Post>
-__device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const cplx<T>* __restrict__ twP, int lt,
-                                           int g, Pre& pre, Post& post) {
+template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, typename TW, typename Pre, typename Post>
+__device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
+                                           Post& post) {
     constexpr int P = 1 << LOGP, TPF = fft_tpf(P), R0 = 1 << (LOGP & 3);
     if constexpr (R0 > 1) {
         constexpr bool LAST = R0 == P;
-        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT>(src, dst, twP, lt, pre, post);
+        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT>(dst, src, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT>(dst, src, tw, lt, g, pre, post);
     } else {
-        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
     }
 }
 
@@ -363,25 +412,25 @@ __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const cpl
 // fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).  ZIN / HOUT
 // as for fft_pass_ct (the generic passes ignore them: they transform and store
 // everything, which is also correct).
-template <typename T, bool INV, bool ZIN = false, bool HOUT = false, typename Pre, typename Post>
-__device__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const cplx<T>* __restrict__ twP, int lt, int tpf,
-                             int g, Pre pre, Post post) {
-    if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
+template <typename T, bool INV, bool ZIN = false, bool HOUT = false, typename TW, typename Pre, typename Post>
+__device__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const TW& tw, int lt, int tpf, int g, Pre pre,
+                             Post post) {
+    if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
     switch (logP) {
-        case 1: return fft_ct<T, INV, 1, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 2: return fft_ct<T, INV, 2, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 3: return fft_ct<T, INV, 3, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 4: return fft_ct<T, INV, 4, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 5: return fft_ct<T, INV, 5, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 6: return fft_ct<T, INV, 6, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 7: return fft_ct<T, INV, 7, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 8: return fft_ct<T, INV, 8, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 9: return fft_ct<T, INV, 9, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 10: return fft_ct<T, INV, 10, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 11: return fft_ct<T, INV, 11, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 12: return fft_ct<T, INV, 12, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        case 13: return fft_ct<T, INV, 13, ZIN, HOUT>(src, dst, twP, lt, g, pre, post);
-        default: return fft_pow2<T, INV>(src, dst, logP, twP, lt, tpf, g, pre, post);
+        case 1: return fft_ct<T, INV, 1, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 2: return fft_ct<T, INV, 2, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 3: return fft_ct<T, INV, 3, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 4: return fft_ct<T, INV, 4, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 5: return fft_ct<T, INV, 5, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 6: return fft_ct<T, INV, 6, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 7: return fft_ct<T, INV, 7, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 8: return fft_ct<T, INV, 8, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 9: return fft_ct<T, INV, 9, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 10: return fft_ct<T, INV, 10, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 11: return fft_ct<T, INV, 11, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 12: return fft_ct<T, INV, 12, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        case 13: return fft_ct<T, INV, 13, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        default: return fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
     }
 }
 
@@ -394,38 +443,18 @@ __device__ void load_twiddles(cplx<T>* twP, int logP, const cplx<T>* __restrict_
     for (int q = threadIdx.x; q < half; q += blockDim.x) twP[padi(q)] = tw[q * stride];
 }
 
-// e^{-i pi q / n} for 0 <= q < 2n from two small tables: q = 64*hi + lo
-template <typename T>
-struct PhaseTab {
-    const cplx<T>* lo;  // 64 entries
-    const cplx<T>* hi;  // ceil(2n/64) entries
-    __device__ __forceinline__ cplx<T> operator()(int q) const { return cmul(hi[q >> 6], lo[q & 63]); }
-};
-
-template <typename T>
-__device__ void build_phase_tab(cplx<T>* lo, cplx<T>* hi, int n) {
-    const int nhi = (2 * n + 63) / 64;
-    for (int i = threadIdx.x; i < 64 + nhi; i += blockDim.x) {
-        int q = i < 64 ? i : 64 * (i - 64);
-        double s, c;
-        sincospi(-(double)q / (double)n, &s, &c);
-        cplx<T> v = {(T)c, (T)s};
-        if (i < 64) lo[i] = v; else hi[i - 64] = v;
-    }
-}
-
 // Complex DFT of length h of buf (natural order, h entries written by this
 // group), forward (e^-) or inverse (e^+); returns the buffer with Z in natural order.
-template <typename T>
-__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const cplx<T>* __restrict__ twP,
+template <typename T, typename TW>
+__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const TW& tw,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp, bool inv, int lt,
                              int tpf, int g) {
     group_sync(tpf, g);
     IdentityMap id;
     if (rp.logh >= 0) {
         if (rp.logh == 0) return buf;
-        return inv ? fft_ring<T, true>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id)
-                   : fft_ring<T, false>(buf, buf2, rp.logh, twP, lt, tpf, g, id, id);
+        return inv ? fft_ring<T, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
+                   : fft_ring<T, false>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id);
     }
     // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
     // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
@@ -448,9 +477,9 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         return v;
     };
     // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
-    cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, twP, lt, tpf, g, pre, mulG);
+    cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
     cplx<T>* o = (r == buf) ? buf2 : buf;
-    return fft_ring<T, true, false, true>(r, o, rp.logP, twP, lt, tpf, g, id, postc);
+    return fft_ring<T, true, false, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
 }
 
 // One complex element (8 or 16 bytes) global -> shared, asynchronously.
@@ -483,12 +512,12 @@ __device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg,
 // Returns the largest |re|, |im| this thread wrote.
 template <typename T, typename Next>
 __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ F, const RingPair& rp,
-                          const cplx<T>* __restrict__ twP, const cplx<T>* __restrict__ gtab,
+                          const PhaseTab<T>& tw, const cplx<T>* __restrict__ gtab,
                           const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g,
                           Next load_next) {
     const int h = rp.h;
     cp_async_wait<0>();
-    cplx<T>* Z = ring_dft(cur, other, rp, twP, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
+    cplx<T>* Z = ring_dft(cur, other, rp, tw, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (Z == cur) ? other : cur;
     load_next(freeb);
     T mx = (T)0;
@@ -533,7 +562,7 @@ __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restri
 // next input.  ref != nullptr: write ref - x (Jacobi residual).
 template <typename T, typename Next>
 __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ x,
-                             const T* __restrict__ ref, const RingPair& rp, const cplx<T>* __restrict__ twP,
+                             const T* __restrict__ ref, const RingPair& rp, const PhaseTab<T>& tw,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
                              const PhaseTab<T>& E, int lt, int tpf, int g, Next load_next) {
     const int h = rp.h, mt = rp.mt;
@@ -560,7 +589,7 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
         buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
         if (k != 0 && kb != k) buf[padi(kb)] = {sum.re + r.im, r.re - sum.im};
     }
-    cplx<T>* z = ring_dft(buf, cur, rp, twP, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
+    cplx<T>* z = ring_dft(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
     load_next(freeb);
     for (int j = lt; j < h; j += tpf) {
