@@ -285,10 +285,10 @@ def run_gpu(args):
         raise RuntimeError(f"timed transform disagrees with the FP32 path: rel-L2 {check_rel:.3e}")
     ms_step = ms / args.steps
     value = world * B * args.steps / (ms / 1000.0)
-    launches_per_step = sum(v[0] for v in stats.values()) / args.steps
+    launches_per_step = sum(v[0] * kernels_in_stage(k, prec) for k, v in stats.items()) / args.steps
 
     # roofline of the dominant kernel
-    roof = roofline(stats, args, prec, refine, nside, L, B)
+    roof = roofline(stats, args, prec, refine, nside, L, B, plan.table_bytes > 0)
 
     # plain FP32 comparison (the target is >= 2x this on the same GPU)
     plain = None
@@ -462,75 +462,106 @@ def _tc_available(hpx, dev):
 
 
 def algorithmic(nside, L, M):
-    """Useful FLOPs of one Legendre contraction direction per map (folded, truncated)
-    and algorithmic bytes of one ring-FFT direction per map."""
-    flops = 0
+    """Per map: useful FLOPs of one Legendre contraction direction (N/S folded,
+    triangle l >= m, each order stopped at its ring's truncation) and the
+    algorithmic HBM bytes of every stage of the step (each operand read once,
+    each result written once).  The table-driven contractions also stream the
+    part of the resident fp16 hi/lo Legendre table they use once per launch:
+    4 bytes per (ring pair, m, l), which equals the FLOP count per map."""
     NP = 2 * nside
+
+    def nphi(tn):
+        return 4 * (tn + 1) if tn < nside - 1 else 4 * nside
+
+    flops = 0
+    kept_pairs = 0
     for p in range(NP):
-        nphi = 4 * (p + 1) if p < nside - 1 else 4 * nside
-        mt = min(M, nphi // 2 + 1)
-        ms = np.arange(mt)
-        flops += 4 * int(np.sum(np.maximum(L - ms, 0)))
-    npix = 12 * nside * nside
+        mt = min(M, nphi(p) // 2 + 1)
+        kept_pairs += mt
+        flops += 4 * int(np.sum(np.maximum(L - np.arange(mt), 0)))
     kept = 0
     for t in range(4 * nside - 1):
-        tn = t if t < NP else 4 * nside - 2 - t
-        nphi = 4 * (tn + 1) if tn < nside - 1 else 4 * nside
-        kept += min(M, nphi // 2 + 1)
-    fft_bytes = 4 * npix + 8 * kept
-    return flops, fft_bytes
+        kept += min(M, nphi(t if t < NP else 4 * nside - 2 - t) // 2 + 1)
+    npix = 12 * nside * nside
+    tri = sum(L - m for m in range(M))
+    stage_bytes = {
+        "ring_fft_forward": 4 * npix + 8 * kept,  # real rings in, ring spectra out
+        "ring_fft_inverse": 8 * kept + 4 * npix,
+        "fold": 8 * kept + 16 * kept_pairs,  # spectra in, fp16 hi/lo S and D per (m, ring pair) out
+        "unfold": 16 * kept_pairs + 8 * kept,  # E and O per (m, ring pair) in, spectra out
+        "legendre_forward": 16 * kept_pairs + 8 * tri,  # operand in, order-major rows out (+ table)
+        "columns_to_alm": 8 * tri + 8 * L * M,  # rows in, dense alm out
+        "alm_to_columns": 16 * L * M + 8 * tri,  # max scan and read of alm, fp16 hi/lo operand out
+        "legendre_inverse": 8 * tri + 16 * kept_pairs,  # operand in, E and O out (+ table)
+    }
+    return flops, stage_bytes
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per full launch of the
-# dominant kernel, from one single-pass ncu capture of this script's default
-# workload: (stage, nside, lmax, precision) -> bytes
-MEASURED_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per 64-map launch of
+# each stage's kernels at nside 1024, lmax = mmax = 2047, f16x3 with the resident
+# table, from one single-pass ncu capture of this script's default workload:
+# stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
+MEASURED_TRAFFIC = {
+    "ring_fft_forward": 3634162688 + 3442558208,
+    "ring_fft_inverse": 3636217856 + 3470151680,
+    "fold": 3222771712 + 3174716160,
+    "legendre_forward": 19722016768 + 1070631680,
+    "columns_to_alm": 1080372224 + 2097201664,
+    "alm_to_columns": (2146283008 + 108544) + (2145484032 + 1078057984),
+    "legendre_inverse": 17335838720 + 3165497088,
+    "unfold": 3224604928 + 3169508608,
+}
+
+# kernels behind each stage's timer (the mixed path's alm_to_columns is a max
+# scan plus the conversion when the operand carries a per-map fp16 scale)
+def kernels_in_stage(name, prec):
+    return 2 if (name == "alm_to_columns" and prec == "f16x3") else 1
 
 
-def roofline(stats, args, prec, refine, nside, L, B):
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
-    flops_map, fft_bytes_map = algorithmic(nside, L, L)
-    dom = max(stats.items(), key=lambda kv: kv[1][1])
-    name, (n, tot) = dom
-    per_launch_ms = tot / max(n, 1)
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        pk = json.load(open(path))
+        return pk.get("hbm_gbs", 6650.0), pk.get("bf16_tflops", 1590.0), "MEASURED_PEAKS.json (measured)"
+    return 6650.0, 1590.0, "fallback (no MEASURED_PEAKS.json): 6650 GB/s and 1590 TFLOP/s, an earlier measurement on this pool"
+
+
+def roofline(stats, args, prec, refine, nside, L, B, table):
+    """Roofline of every timed stage and of the dominant one (largest time).
+    Table-driven contractions stream their operands and the resident table and
+    are HBM-bound; their tensor-core rate is reported beside it."""
+    hbm, bf16, source = load_peaks()
+    flops_map, stage_bytes = algorithmic(nside, L, L)
     chunk = min(B, 64)
-    if name.startswith("legendre"):
-        useful = flops_map * chunk
-        if prec in ("bf16x3", "f16x3", "tf32"):
-            terms = 1 if prec == "tf32" else 3
-            # fp16 and bf16 run at the same tcgen05 kind::f16 rate
-            peak = peaks.get("bf16_tflops", 1590.0) if prec != "tf32" else peaks.get("bf16_tflops", 1590.0) / 2
-            achieved = useful * terms / (per_launch_ms * 1e-3) / 1e12
-            traffic = MEASURED_TRAFFIC.get((name, nside, L, prec)) if B >= 64 else None
-            return {
-                "kernel": name,
-                "bound": "tensor",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "TFLOP/s",
-                "frac": achieved / peak,
-                "traffic": traffic,
-                "traffic_unit": "bytes per launch",
-                "useful_tflops": useful / (per_launch_ms * 1e-3) / 1e12,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" + ("; tf32 taken as half" if prec == "tf32" else ""),
-            }
-        achieved = useful / (per_launch_ms * 1e-3) / 1e12
-        peak = FP32_SIMT_PEAK_TFLOPS
-        return {
-            "kernel": name,
-            "bound": "fp32_simt",
-            "achieved": achieved,
-            "peak": peak,
-            "unit": "TFLOP/s",
-            "frac": achieved / peak,
-            "traffic": None,
-            "peak_source": "nominal FP32 FMA rate: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz",
-        }
-    byts = fft_bytes_map * chunk
-    achieved = byts / (per_launch_ms * 1e-3) / 1e9
-    peak = peaks.get("hbm_gbs", 6650.0)
-    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None}
+    measured = nside == 1024 and L == 2047 and prec == "f16x3" and chunk == 64 and table
+    stages = {}
+    for name, (n, tot) in stats.items():
+        if not n:
+            continue
+        ms = tot / n
+        e = {"ms_per_launch": ms}
+        if name.startswith("legendre") and not (prec in ("bf16x3", "f16x3") and table):
+            useful = flops_map * chunk
+            if prec in ("bf16x3", "f16x3"):
+                e.update(bound="tensor", achieved=3 * useful / (ms * 1e-3) / 1e12, peak=bf16, unit="TFLOP/s")
+            else:
+                e.update(bound="fp32_simt", achieved=useful / (ms * 1e-3) / 1e12, peak=FP32_SIMT_PEAK_TFLOPS,
+                         unit="TFLOP/s")
+        else:
+            byts = stage_bytes.get(name, 0) * chunk
+            if name.startswith("legendre"):
+                byts += flops_map
+                e["tensor_tflops"] = 3 * flops_map * chunk / (ms * 1e-3) / 1e12
+                e["tensor_frac"] = e["tensor_tflops"] / bf16
+            e.update(bound="hbm", achieved=byts / (ms * 1e-3) / 1e9, peak=hbm, unit="GB/s", algorithmic_bytes=byts)
+        e["frac"] = e["achieved"] / e["peak"]
+        e["traffic"] = MEASURED_TRAFFIC.get(name) if measured else None
+        stages[name] = e
+    dom = max(stats.items(), key=lambda kv: kv[1][1])[0]
+    d = stages[dom]
+    out = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
+           "frac": d["frac"], "traffic": d["traffic"], "peak_source": source, "stages": stages}
+    return out
 
 
 # FP32 CUDA-core peak of a B200 at its maximum SM clock

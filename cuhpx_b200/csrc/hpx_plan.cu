@@ -67,9 +67,9 @@ int ceil_log2(int v) {
     return r;
 }
 
-enum Stage { kStRingFwd = 0, kStRingInv, kStLegFwd, kStLegInv, kStAlmCols, kStFold, kStUnfold, kNumStages };
+enum Stage { kStRingFwd = 0, kStRingInv, kStLegFwd, kStLegInv, kStAlmCols, kStFold, kStUnfold, kStColsAlm, kNumStages };
 const char* kStageNames[kNumStages] = {"ring_fft_forward", "ring_fft_inverse", "legendre_forward", "legendre_inverse",
-                                       "alm_to_columns",   "fold",             "unfold"};
+                                       "alm_to_columns",   "fold",             "unfold",           "columns_to_alm"};
 
 }  // namespace
 
@@ -822,26 +822,30 @@ struct Pipeline {
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();
-        Timer tm(P, st, kStLegFwd);
         if (P->mixed()) {
             const TcPlan& TP = P->tc;
-            if (!accumulate && TP.m_tc_end < P->M)
-                k_zero_alm_cols<<<1024, 256, 0, st>>>((float*)alm, nb, P->L, P->M, TP.m_tc_end);
-            if (TP.n_fwd_tiles == 0) return;
-            CUtensorMap mh, ml;
-            if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
-            if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
             float* yc = (float*)(P->ycols_in_F() ? (void*)F : (void*)ycols_alt);
-            auto kern = TP.table ? (P->f16() ? k_leg_fwd_tc<true, true> : k_leg_fwd_tc<false, true>)
-                                 : (P->f16() ? k_leg_fwd_tc<true, false> : k_leg_fwd_tc<false, false>);
-            kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(
-                mh, ml, TP.table ? TP.tab_fwd : mh, nb, yc, P->L, P->Lpad, P->geo, P->d_z, P->d_lstart,
-                P->d_lsmax, P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, fmax,
-                fold_wb, TP.d_err);
+            {
+                Timer tm(P, st, kStLegFwd);
+                if (!accumulate && TP.m_tc_end < P->M)
+                    k_zero_alm_cols<<<1024, 256, 0, st>>>((float*)alm, nb, P->L, P->M, TP.m_tc_end);
+                if (TP.n_fwd_tiles == 0) return;
+                CUtensorMap mh, ml;
+                if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
+                if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
+                auto kern = TP.table ? (P->f16() ? k_leg_fwd_tc<true, true> : k_leg_fwd_tc<false, true>)
+                                     : (P->f16() ? k_leg_fwd_tc<true, false> : k_leg_fwd_tc<false, false>);
+                kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(
+                    mh, ml, TP.table ? TP.tab_fwd : mh, nb, yc, P->L, P->Lpad, P->geo, P->d_z, P->d_lstart,
+                    P->d_lsmax, P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_fwd_tiles, TP.d_fwd_off, fmax,
+                    fold_wb, TP.d_err);
+            }
+            Timer tm(P, st, kStColsAlm);
             dim3 tg((TP.m_tc_end + 31) / 32, P->L);
             k_tc_to_alm<<<tg, dim3(32, 8), 0, st>>>(yc, nb, P->L, P->M, TP.m_tc_end, (float*)alm, accumulate);
             return;
         }
+        Timer tm(P, st, kStLegFwd);
         dim3 grid(P->n_fwdtiles, (C + FwdCfg<T>::CT - 1) / FwdCfg<T>::CT);
         k_leg_fwd_simt<T><<<grid, 256, P->fwd_smem, st>>>(spec, C, nb, alm, P->L, P->M, P->geo, P->d_pairs,
                                                           P->d_lstart, P->d_pstart, P->d_coef, P->Lpad, P->d_seeds,
