@@ -74,6 +74,14 @@ __device__ unsigned long long g_tc_prof[2][148 * 2][kTcpSlots];
 
 constexpr int kTcCols = 128;      // N: columns per tile (64 maps)
 constexpr int kTcThreads = 512;   // 16 warps
+// Table-driven epilogues stage each warp's 32 rows x 16 columns in shared
+// memory (row stride 20 floats: the row writes of 8 lanes fall on distinct
+// banks) and store them as 8 rows x 64 contiguous bytes per instruction,
+// instead of one 16-byte piece of each of 32 rows 512 bytes apart.
+constexpr int kEpiStride = 20;
+constexpr int kEpiStageFloats = 32 * kEpiStride;  // per warp
+constexpr int kEpiStageBytes = 8 * kEpiStageFloats * 4;
+
 // analysis: 6 stages of 16 rings (32 KB: A 4 x 4 KB, B 4 x 4 KB)
 constexpr int kFStages = 6;
 constexpr int kFRing = 16;
@@ -86,8 +94,28 @@ constexpr int kIStages = 3;
 constexpr int kIStageBytes = 65536;
 constexpr int kTcInvRings = 128;  // rings per synthesis tile
 constexpr int kTcDegChunk = 64;   // degrees per synthesis stage (32 per parity)
-constexpr int kISmem = kIStages * kIStageBytes + 8 * 64 * 16 + 1024 + 1024;
+constexpr int kISmem = kIStages * kIStageBytes + 8 * 64 * 16 + 1024 + kEpiStageBytes + 1024;
 constexpr int kMaxStages = 6;
+// Epilogue warps (4..4+n): 4 drain both parities; the table-driven kernels have
+// no producer warps, so 8 drain one parity each (warp w reads TMEM lanes
+// 32 (w mod 4) .. +31 either way).
+template <bool TAB>
+constexpr int kEpiWarps = TAB ? 8 : 4;
+// One 32 x 16 block: lane r holds v[0..16) of row r; row r goes to row_ptr(r)
+// (nullptr: skipped).  Ends with the warp's staging buffer free again.
+template <typename RowPtr>
+__device__ __forceinline__ void epi_store_block(float* stg, const float (&v)[16], int lane, RowPtr row_ptr) {
+#pragma unroll
+    for (int j = 0; j < 16; j += 4) *(float4*)(stg + lane * kEpiStride + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = k * 8 + (lane >> 2), q = lane & 3;
+        float* dst = row_ptr(r);
+        if (dst) *(float4*)(dst + 4 * q) = *(const float4*)(stg + r * kEpiStride + 4 * q);
+    }
+    __syncwarp();
+}
 
 // Host-side state of the tensor-core path, owned by the plan.
 struct TcPlan {
@@ -188,7 +216,9 @@ __device__ __forceinline__ void mma_drain(TcShared* sh) {
     tc::mbar_wait_quiet(&sh->drain, 0);
 }
 
-__device__ __forceinline__ void tc_setup(TcShared* sh, int stages, int prod_arrivals, int warp) {
+// acc_arrivals: epilogue warps that drain one accumulator (4, or 8 when the
+// table-driven kernels, which have no producer warps, split the two parities)
+__device__ __forceinline__ void tc_setup(TcShared* sh, int stages, int prod_arrivals, int warp, int acc_arrivals) {
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
             tc::mbar_init(&sh->full_tma[s], 1);
@@ -197,7 +227,7 @@ __device__ __forceinline__ void tc_setup(TcShared* sh, int stages, int prod_arri
         }
         for (int a = 0; a < 2; ++a) {
             tc::mbar_init(&sh->acc_full[a], 1);
-            tc::mbar_init(&sh->acc_empty[a], 4);
+            tc::mbar_init(&sh->acc_empty[a], acc_arrivals);
         }
         tc::mbar_init(&sh->drain, 1);
         tc::fence_mbar_init();
@@ -395,7 +425,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int nbk = seed_blocks(L);
     const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, fmax, wb, nmaps);
-    tc_setup(sh, kFStages, 1, warp);
+    tc_setup(sh, kFStages, 1, warp, kEpiWarps<TAB>);
     const uint32_t tmem = sh->tmem_base;
     auto nchunks = [&](int m) { return (NP - geo.first_ring(m) + kFRing - 1) / kFRing; };
 
@@ -483,13 +513,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             TCP_ADD(0, 10, role);
             TCP_FLUSH(0);
         }
-    } else if (warp >= 4 && warp < 8) {
+    } else if (warp >= 4 && warp < 4 + kEpiWarps<TAB>) {
         // ------------------------------------------------ epilogue: TMEM -> ycols[m][l][128]
         // Each row (m, l) is written whole by one thread (512 contiguous bytes),
         // so no two CTAs write the same sector; k_tc_to_alm scatters the rows
         // into alm[b][l][m] with coalesced stores.
         TCP_DECL;
         const int ew = warp & 3;  // TMEM lanes 32*ew .. +31
+        const int par_lo = kEpiWarps<TAB> == 8 ? (warp - 4) >> 2 : 0;
+        const int par_hi = kEpiWarps<TAB> == 8 ? par_lo + 1 : 2;
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, jb = tiles[t].y;
@@ -501,7 +533,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tc::tc_fence_after();
             const int row = ew * 32 + lane;
 #pragma unroll 1
-            for (int par = 0; par < 2; ++par) {
+            for (int par = par_lo; par < par_hi; ++par) {
                 const int l = l0 + 2 * row + par;
                 const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + par * 2 * kTcCols;
 #pragma unroll 1
@@ -511,7 +543,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     tc::tmem_ld16(taddr + kTcCols + c, w);
 #pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] += w[j];
-                    if (l < L) {
+                    if constexpr (TAB) {
+#pragma unroll
+                        for (int j = 0; j < 16; j += 2) {
+                            const float sc = s_inv[(c + j) >> 1];
+                            v[j] *= sc;
+                            v[j + 1] *= sc;
+                        }
+                        float* stg = (float*)coef_s + (warp - 4) * kEpiStageFloats;
+                        const int lr0 = l0 + 2 * ew * 32 + par;  // degree of row 0 of this warp
+                        epi_store_block(stg, v, lane, [&](int r) -> float* {
+                            const int lr = lr0 + 2 * r;
+                            return lr < L ? ycols + ((int64_t)m * L + lr) * kTcCols + c : nullptr;
+                        });
+                    } else if (l < L) {
                         float* dst = ycols + ((int64_t)m * L + l) * kTcCols + c;
 #pragma unroll
                         for (int j = 0; j < 16; j += 4) {
@@ -677,12 +722,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     unsigned char* stages = base;
     AlphaC* coef_s = (AlphaC*)(base + kIStages * kIStageBytes);
     TcShared* sh = (TcShared*)(base + kIStages * kIStageBytes + 8 * 64 * 16);
+    float* epi_stage = (float*)(base + kIStages * kIStageBytes + 8 * 64 * 16 + 1024);  // table mode
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NP = geo.NP;
     const int nbk = seed_blocks(L);
     const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, amax, 1.f, nmaps);
-    tc_setup(sh, kIStages, 2, warp);
+    tc_setup(sh, kIStages, 2, warp, kEpiWarps<TAB>);
     const uint32_t tmem = sh->tmem_base;
     auto nchunks = [&](int m) { return m < L ? (L - m + kTcDegChunk - 1) / kTcDegChunk : 0; };
 
@@ -771,10 +817,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             TCP_ADD(1, 10, role);
             TCP_FLUSH(1);
         }
-    } else if (warp >= 4 && warp < 8) {
+    } else if (warp >= 4 && warp < 4 + kEpiWarps<TAB>) {
         // ------------------------------------------------ epilogue: TMEM -> spec (E, O)
         TCP_DECL;
-        const int ew = warp & 3;
+        const int ew = warp & 3;  // TMEM lanes 32*ew .. +31
+        const int par_lo = kEpiWarps<TAB> == 8 ? (warp - 4) >> 2 : 0;
+        const int par_hi = kEpiWarps<TAB> == 8 ? par_lo + 1 : 2;
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
             const int m = tiles[t].x, rb = tiles[t].y;
@@ -787,7 +835,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             TCP_T0(e1);
             tc::tc_fence_after();
 #pragma unroll 1
-            for (int par = 0; par < 2; ++par) {
+            for (int par = par_lo; par < par_hi; ++par) {
                 float* dst = spec + (((int64_t)m * 2 + par) * NP + p) * C;
                 const uint32_t taddr = tmem + ((uint32_t)(ew * 32) << 16) + par * 2 * kTcCols;
 #pragma unroll 1
@@ -797,7 +845,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     tc::tmem_ld16(taddr + kTcCols + c, w);
 #pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] += w[j];
-                    if (p < NP && c < C) {
+                    if constexpr (TAB) {
+#pragma unroll
+                        for (int j = 0; j < 16; j += 2) {
+                            const float sc = s_inv[(c + j) >> 1];
+                            v[j] *= sc;
+                            v[j + 1] *= sc;
+                        }
+                        float* stg = epi_stage + (warp - 4) * kEpiStageFloats;
+                        const int p0 = t0 + rb + ew * 32;  // ring of row 0 of this warp
+                        float* base0 = spec + (((int64_t)m * 2 + par) * NP) * C + c;
+                        epi_store_block(stg, v, lane, [&](int r) -> float* {
+                            return (p0 + r < NP && c < C) ? base0 + (int64_t)(p0 + r) * C : nullptr;
+                        });
+                    } else if (p < NP && c < C) {
 #pragma unroll
                         for (int j = 0; j < 16; j += 4) {
                             const float s0 = s_inv[(c + j) >> 1], s1 = s_inv[((c + j) >> 1) + 1];
