@@ -307,7 +307,7 @@ int tc_table_create(hpx_plan_s* P) {
                                                P->d_pstart, P->d_coef, P->d_seeds, T.d_table);
     HPX_CUDA_TRY(cudaGetLastError());
     HPX_CUDA_TRY(cudaDeviceSynchronize());
-    int rc = encode_table(P, &T.tab_fwd, 64, kFRing, CU_TENSOR_MAP_SWIZZLE_128B);
+    int rc = encode_table(P, &T.tab_fwd, 64, kFRingS<true>, CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc != HPX_OK) return rc;
     rc = encode_table(P, &T.tab_inv, kTcDegChunk / 2, kTcInvRings, CU_TENSOR_MAP_SWIZZLE_64B);
     if (rc != HPX_OK) return rc;
@@ -831,8 +831,9 @@ struct Pipeline {
                     k_zero_alm_cols<<<1024, 256, 0, st>>>((float*)alm, nb, P->L, P->M, TP.m_tc_end);
                 if (TP.n_fwd_tiles == 0) return;
                 CUtensorMap mh, ml;
-                if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
-                if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, kFRing)) != HPX_OK) return;
+                const int box_rings = TP.table ? kFRingS<true> : kFRingS<false>;
+                if ((rc = encode_operand(P, &mh, xh(), P->NP, 2ull * P->M, box_rings)) != HPX_OK) return;
+                if ((rc = encode_operand(P, &ml, xl(), P->NP, 2ull * P->M, box_rings)) != HPX_OK) return;
                 auto kern = TP.table ? (P->f16() ? k_leg_fwd_tc<true, true> : k_leg_fwd_tc<false, true>)
                                      : (P->f16() ? k_leg_fwd_tc<true, false> : k_leg_fwd_tc<false, false>);
                 kern<<<TP.n_fwd_ctas, kTcThreads, kFSmem, st>>>(

@@ -89,6 +89,16 @@ constexpr int kFStageBytes = 32768;
 constexpr int kTcFwdDeg = 256;    // degrees per analysis tile (128 per parity)
 constexpr int kFCoef = 256;       // per-producer-warp coefficient window (AlphaC)
 constexpr int kFSmem = kFStages * kFStageBytes + 8 * kFCoef * 16 + 1024 + 1024;
+// The table-driven analysis runs the same 192 KB as 3 stages of 32 rings
+// (4 KB TMA boxes, two K-steps of 16 rings per stage): half the boxes, barrier
+// round trips and commits per byte.  Producer-fed stages stay at 16 rings.
+template <bool TAB>
+constexpr int kFRingS = TAB ? 32 : kFRing;
+template <bool TAB>
+constexpr int kFStagesS = TAB ? 3 : kFStages;
+template <bool TAB>
+constexpr int kFStageBytesS = TAB ? 65536 : kFStageBytes;
+static_assert(kFStagesS<true> * kFStageBytesS<true> == kFStages * kFStageBytes, "same stage memory");
 // synthesis: 3 stages of 64 degrees (64 KB: A 4 x 8 KB, B 4 x 8 KB)
 constexpr int kIStages = 3;
 constexpr int kIStageBytes = 65536;
@@ -425,9 +435,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int nbk = seed_blocks(L);
     const int t_begin = tile_off[blockIdx.x], t_end = tile_off[blockIdx.x + 1];  // this CTA's tiles
     load_inv_scales<F16>(s_inv, fmax, wb, nmaps);
-    tc_setup(sh, kFStages, 1, warp, kEpiWarps<TAB>);
+    tc_setup(sh, kFStagesS<TAB>, 1, warp, kEpiWarps<TAB>);
     const uint32_t tmem = sh->tmem_base;
-    auto nchunks = [&](int m) { return (NP - geo.first_ring(m) + kFRing - 1) / kFRing; };
+    constexpr int RS = kFRingS<TAB>, NS = kFStagesS<TAB>, SB = kFStageBytesS<TAB>;
+    // stage s: A (Pbar) at s SB, B (operand) at s SB + SB/2; within each, the
+    // (par, hl) blocks are SB/8 apart and their two 64-wide halves SB/16 apart
+    auto nchunks = [&](int m) { return (NP - geo.first_ring(m) + RS - 1) / RS; };
 
     if (warp == 0) {
         if (lane == 0) {
@@ -440,33 +453,33 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int t0 = geo.first_ring(m);
                 const int nch = nchunks(m);
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kFStages;
-                    if (!tc::mbar_wait(&sh->empty[s], ((it / kFStages) & 1) ^ 1, err, 11)) goto tma_done;
-                    unsigned char* st = stages + s * kFStageBytes + 16384;
-                    tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? 32768 : 16384);
-                    const int y = t0 + c * kFRing;
+                    const int s = it % NS;
+                    if (!tc::mbar_wait(&sh->empty[s], ((it / NS) & 1) ^ 1, err, 11)) goto tma_done;
+                    unsigned char* st = stages + s * SB + SB / 2;
+                    tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? SB : SB / 2);
+                    const int y = t0 + c * RS;  // rings past NP read as zeros (TMA out-of-bounds fill)
                     if (TAB) {
-                        // A operand: Pbar for 128 degrees of each parity x 16 rings, hi and lo
+                        // A operand: Pbar for 128 degrees of each parity x RS rings, hi and lo
 #pragma unroll
                         for (int ph = 0; ph < 4; ++ph)
 #pragma unroll
                             for (int h = 0; h < 2; ++h)
-                                tc::tma_load_3d(stages + s * kFStageBytes + ph * 4096 + h * 2048, &tab_map,
+                                tc::tma_load_3d(stages + s * SB + ph * (SB / 8) + h * (SB / 16), &tab_map,
                                                 jb * (kTcFwdDeg / 2) + h * 64, y, 4 * m + ph, &sh->full_tma[s]);
                     }
 #pragma unroll
                     for (int par = 0; par < 2; ++par)
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
-                            tc::tma_load_3d(st + (par * 2 + 0) * 4096 + h * 2048, &xh_map, h * 64, y, 2 * m + par,
-                                            &sh->full_tma[s]);
-                            tc::tma_load_3d(st + (par * 2 + 1) * 4096 + h * 2048, &xl_map, h * 64, y, 2 * m + par,
-                                            &sh->full_tma[s]);
+                            tc::tma_load_3d(st + (par * 2 + 0) * (SB / 8) + h * (SB / 16), &xh_map, h * 64, y,
+                                            2 * m + par, &sh->full_tma[s]);
+                            tc::tma_load_3d(st + (par * 2 + 1) * (SB / 8) + h * (SB / 16), &xl_map, h * 64, y,
+                                            2 * m + par, &sh->full_tma[s]);
                         }
                 }
             }
         tma_done:
-            tma_drain(sh, it, kFStages);
+            tma_drain(sh, it, NS);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -482,8 +495,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 TCP_ADD(0, 2, w2);
                 tc::tc_fence_after();
                 for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % kFStages;
-                    const uint32_t ph = (it / kFStages) & 1;
+                    const int s = it % NS;
+                    const uint32_t ph = (it / NS) & 1;
                     TCP_T0(w0);
                     if (!tc::mbar_wait(&sh->full_tma[s], ph, err, 13)) goto mma_done;
                     TCP_ADD(0, 0, w0);
@@ -491,18 +504,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!TAB && !tc::mbar_wait(&sh->full_prod[s], ph, err, 14)) goto mma_done;
                     TCP_ADD(0, 1, w1);
                     tc::tc_fence_after();
-                    const uint32_t sa = tc::smem_u32(stages + s * kFStageBytes);
-                    const uint32_t sb = sa + 16384;
+                    const uint32_t sa = tc::smem_u32(stages + s * SB);
+                    const uint32_t sb = sa + SB / 2;
 #pragma unroll
                     for (int par = 0; par < 2; ++par) {
                         const uint32_t dm = tmem + par * 2 * kTcCols, dc = dm + kTcCols;
-                        const uint64_t ah = tc::smem_desc_sw128(sa + (par * 2 + 0) * 4096, 2048, 1024);
-                        const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * 4096, 2048, 1024);
-                        const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 4096, 2048, 1024);
-                        const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 4096, 2048, 1024);
-                        tc::mma_bf16(dm, ah, bh, idesc, c > 0 ? 1u : 0u);
-                        tc::mma_bf16(dc, ah, bl, idesc, c > 0 ? 1u : 0u);
-                        tc::mma_bf16(dc, al, bh, idesc, 1u);
+#pragma unroll
+                        for (int ks = 0; ks < RS / 16; ++ks) {
+                            // K-step ks: rings 16 ks .. +15, 16 rows of 128 B into each 64-wide half
+                            const uint32_t ko = ks * 2048;
+                            const uint64_t ah = tc::smem_desc_sw128(sa + (par * 2 + 0) * (SB / 8) + ko, SB / 16, 1024);
+                            const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * (SB / 8) + ko, SB / 16, 1024);
+                            const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * (SB / 8) + ko, SB / 16, 1024);
+                            const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * (SB / 8) + ko, SB / 16, 1024);
+                            const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+                            tc::mma_bf16(dm, ah, bh, idesc, acc);
+                            tc::mma_bf16(dc, ah, bl, idesc, acc);
+                            tc::mma_bf16(dc, al, bh, idesc, 1u);
+                        }
                     }
                     tc::mma_commit(&sh->empty[s]);
                 }
