@@ -388,6 +388,21 @@ int tc_create(hpx_plan_s* P) {
 
 // 3-D tensor map of 2-byte elements (bf16 or fp16 halves; TMA only moves bytes) over
 // [outer][rows][128 cols] with a {64 cols, box_rows} box, 128B swizzle.
+// spec[2M][NP][C] (FP32) for the synthesis epilogue's TMA stores: boxes of
+// 16 columns x 32 rings in the 64-byte swizzle
+int encode_spec_store(const hpx_plan_s* P, CUtensorMap* map, void* spec) {
+    const cuuint64_t C = (cuuint64_t)P->cols();
+    const cuuint64_t dims[3] = {C, (cuuint64_t)P->NP, 2ull * P->M};
+    const cuuint64_t strides[2] = {C * 4, C * 4 * P->NP};
+    const cuuint32_t box[3] = {16, 32, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = ((EncodeTiledFn)P->tc.encode)(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, spec, dims, strides, box, es,
+                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                               CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(HPX_ERR_CUDA, "cuTensorMapEncodeTiled (spec) failed: " + std::to_string((int)r));
+    return HPX_OK;
+}
+
 int encode_operand(const hpx_plan_s* P, CUtensorMap* map, void* base, uint64_t rows, uint64_t outer, int box_rows) {
     const cuuint64_t dims[3] = {(cuuint64_t)kTcCols, rows, outer};
     const cuuint64_t strides[2] = {(cuuint64_t)kTcCols * 2, (cuuint64_t)kTcCols * 2 * rows};
@@ -878,10 +893,12 @@ struct Pipeline {
             CUtensorMap mh, ml;
             if ((rc = encode_operand(P, &mh, ah, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
             if ((rc = encode_operand(P, &ml, al, TP.Lh, 2ull * P->M, 32)) != HPX_OK) return;
+            CUtensorMap sm = mh;
+            if (TP.table && (rc = encode_spec_store(P, &sm, spec)) != HPX_OK) return;
             auto kern = TP.table ? (P->f16() ? k_leg_inv_tc<true, true> : k_leg_inv_tc<false, true>)
                                  : (P->f16() ? k_leg_inv_tc<true, false> : k_leg_inv_tc<false, false>);
             kern<<<TP.n_inv_ctas, kTcThreads, kISmem, st>>>(
-                mh, ml, TP.table ? TP.tab_inv : mh, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->geo, P->d_z, P->d_lstart, P->d_lsmax,
+                mh, ml, TP.table ? TP.tab_inv : mh, sm, (float*)spec, C, nb, P->L, P->M, P->Lpad, P->geo, P->d_z, P->d_lstart, P->d_lsmax,
                 P->d_pstart, P->d_coef, P->d_alphac, P->d_seeds, TP.d_inv_tiles, TP.d_inv_off, amax, TP.d_err);
             return;
         }

@@ -728,7 +728,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 template <bool F16, bool TAB>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_leg_inv_tc(const __grid_constant__ CUtensorMap ah_map, const __grid_constant__ CUtensorMap al_map,
-                 const __grid_constant__ CUtensorMap tab_map,
+                 const __grid_constant__ CUtensorMap tab_map, const __grid_constant__ CUtensorMap spec_map,
                  float* __restrict__ spec, int C, int nmaps, int L, int M, int Lpad, Geom geo,
                  const double* __restrict__ zr, const int* __restrict__ lstart, const int* __restrict__ lsmax,
                  const double2* __restrict__ pstart, const double2* __restrict__ coef,
@@ -871,12 +871,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             v[j] *= sc;
                             v[j + 1] *= sc;
                         }
-                        float* stg = epi_stage + (warp - 4) * kEpiStageFloats;
-                        const int p0 = t0 + rb + ew * 32;  // ring of row 0 of this warp
-                        float* base0 = spec + (((int64_t)m * 2 + par) * NP) * C + c;
-                        epi_store_block(stg, v, lane, [&](int r) -> float* {
-                            return (p0 + r < NP && c < C) ? base0 + (int64_t)(p0 + r) * C : nullptr;
-                        });
+                        // the warp's 32 rings x 16 columns, dense in the 64-byte swizzle of
+                        // spec_map, go out as one TMA store (rings past NP are clipped)
+                        unsigned char* stg = (unsigned char*)(epi_stage + (warp - 4) * kEpiStageFloats);
+                        if (lane == 0) tc::bulk_wait_read0();  // the previous store has read the buffer
+                        __syncwarp();
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            *(float4*)(stg + tc::sw64_offset(lane, j)) =
+                                make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                        tc::fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) {
+                            tc::tma_store_3d(&spec_map, stg, c, t0 + rb + ew * 32, 2 * m + par);
+                            tc::bulk_commit();
+                        }
                     } else if (p < NP && c < C) {
 #pragma unroll
                         for (int j = 0; j < 16; j += 4) {
@@ -891,6 +900,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane == 0) tc::mbar_arrive(&sh->acc_empty[0]);
             if (lane == 0) TCP_ADD(1, 6, e1);
         }
+        if (TAB && lane == 0) tc::bulk_wait0();  // every TMA store of this warp is done
         if (lane == 0) TCP_FLUSH(1);
     } else if (!TAB && warp >= 8 && warp < 8 + 2 * kIStages) {
         // ------------------------------------------------ Pbar^T producers
