@@ -115,27 +115,33 @@ __global__ void __launch_bounds__(256, ring_min_ctas<T>())
     }
 }
 
-// Per-map max |x| over rows of n floats: atomicMax of the float bits into out[map]
-// (out zeroed by the caller).  Grid (blocks per row, maps).
-__global__ void __launch_bounds__(256) k_rows_maxabs(const float* __restrict__ x, int64_t n,
-                                                     unsigned* __restrict__ out) {
-    const int b = blockIdx.y;
-    const float* row = x + (int64_t)b * n;
+// Per-map max |a| over the coefficients the synthesis uses, a[b][l][m] for
+// m <= l (complex, 8-byte aligned): atomicMax of the float bits into out[b]
+// (out zeroed by the caller).  Grid (ceil(L/8), maps); warp w scans row
+// l = 8 blockIdx.x + w.
+__global__ void __launch_bounds__(256) k_alm_maxabs(const float* __restrict__ alm, int L, int M,
+                                                    unsigned* __restrict__ out) {
+    const int b = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int l = blockIdx.x * 8 + warp;
     float v = 0.f;
-    const int64_t n4 = ((((uintptr_t)row) & 15) == 0) ? n / 4 : 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
-        const float4 q = *(const float4*)(row + 4 * i);
-        v = fmaxf(v, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)), fmaxf(fabsf(q.z), fabsf(q.w))));
+    if (l < L) {
+        const int n = min(l + 1, M);
+        const float2* row = (const float2*)(alm + 2 * (((int64_t)b * L + l) * M));
+        int m = lane;
+        for (; m + 96 < n; m += 128) {
+            const float2 q0 = row[m], q1 = row[m + 32], q2 = row[m + 64], q3 = row[m + 96];
+            v = fmaxf(v, fmaxf(fmaxf(fabsf(q0.x), fabsf(q0.y)), fmaxf(fabsf(q1.x), fabsf(q1.y))));
+            v = fmaxf(v, fmaxf(fmaxf(fabsf(q2.x), fabsf(q2.y)), fmaxf(fabsf(q3.x), fabsf(q3.y))));
+        }
+        for (; m < n; m += 32) v = fmaxf(v, fmaxf(fabsf(row[m].x), fabsf(row[m].y)));
     }
-    for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v = fmaxf(v, fabsf(row[i]));
 #pragma unroll
     for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     __shared__ float red[8];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    if (lane == 0) red[warp] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = fmaxf(v, red[w]);
+        for (int w = 1; w < 8; ++w) v = fmaxf(v, red[w]);
         if (v > 0.f) atomicMax(out + b, __float_as_uint(v));
     }
 }
@@ -156,26 +162,44 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
                                               int C, uint32_t* __restrict__ xh, uint32_t* __restrict__ xl,
                                               const unsigned* __restrict__ fmax, float wb) {
     constexpr int MB = fold_mb<T>();
+    constexpr int NL = 64 * MB / 256;  // elements per thread (the kernel runs 256 threads)
     __shared__ cplx<T> tn[64][MB + 1];
     __shared__ cplx<T> ts[64][MB + 1];
+    __shared__ float s_sc[64];
     const int NP = geo.NP;
     const int m0 = blockIdx.x * MB, p = blockIdx.y, bz = blockIdx.z * 64;
     const RingPair rp = pairs[p];
     if (m0 >= rp.mt) return;
     const int tid = threadIdx.x;
-    for (int i = tid; i < 64 * MB; i += blockDim.x) {
-        const int b = bz + i / MB, mm = i % MB, m = m0 + mm;
-        cplx<T> vn = {(T)0, (T)0}, vs = {(T)0, (T)0};
+    // all loads of the thread are issued before the first shared-memory store
+    cplx<T> vn[NL], vs[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
+        const int b = bz + i / MB, m = m0 + i % MB;
+        vn[k] = {(T)0, (T)0};
+        vs[k] = {(T)0, (T)0};
         if (b < nmaps && m < rp.mt) {
-            vn = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m));
-            if (rp.has_south) vs = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m));
+            vn[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m));
+            if (rp.has_south) vs[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m));
         }
-        tn[b - bz][mm] = vn;
-        ts[b - bz][mm] = vs;
+    }
+    if (xh && fmax && tid < 64) {
+        // FP16 operands scaled by 2^e(map); |S|, |D| <= wb * max|F|
+        const int b = bz + tid;
+        s_sc[tid] = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? fmax[b] : 0u) * wb));
+    }
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
+        tn[i / MB][i % MB] = vn[k];
+        ts[i / MB][i % MB] = vs[k];
     }
     __syncthreads();
     // each thread: one (m, map) pair -> S and D
-    for (int i = tid; i < MB * 64; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
         const int mm = i >> 6, bl = i & 63, b = bz + bl, m = m0 + mm;
         if (m >= rp.mt || 2 * b >= C) continue;
         const T wk = adjoint ? ((m == 0 || m == rp.h) ? (T)1 : (T)2) : (T)rp.w;
@@ -191,8 +215,7 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
         const int64_t i0 = (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b;
         const int64_t i1 = (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b;
         if (xh && fmax) {
-            // FP16 operands scaled by 2^e(map); |S|, |D| <= wb * max|F|
-            const float sc = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? fmax[b] : 0u) * wb));
+            const float sc = s_sc[bl];
             uint16_t h0, l0, h1, l1;
             tc::split_f16((float)S.re * sc, h0, l0);
             tc::split_f16((float)S.im * sc, h1, l1);
@@ -227,6 +250,7 @@ __global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int 
                                                 const RingPair* __restrict__ pairs, int adjoint, T* __restrict__ F,
                                                 int64_t Ftot) {
     constexpr int MB = fold_mb<T>();
+    constexpr int NL = 64 * MB / 256;  // elements per thread (the kernel runs 256 threads)
     __shared__ cplx<T> te[MB][65];
     __shared__ cplx<T> to[MB][65];
     const int NP = geo.NP;
@@ -234,18 +258,29 @@ __global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int 
     const RingPair rp = pairs[p];
     if (m0 >= rp.mt) return;
     const int tid = threadIdx.x;
-    for (int i = tid; i < MB * 64; i += blockDim.x) {
+    // all loads of the thread are issued before the first shared-memory store
+    cplx<T> ve[NL], vo[NL];
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
         const int mm = i >> 6, bl = i & 63, b = bz + bl, m = m0 + mm;
-        cplx<T> e = {(T)0, (T)0}, o = {(T)0, (T)0};
+        ve[k] = {(T)0, (T)0};
+        vo[k] = {(T)0, (T)0};
         if (m < rp.mt && 2 * b < C) {
-            e = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b);
-            o = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b);
+            ve[k] = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b);
+            vo[k] = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b);
         }
-        te[mm][bl] = e;
-        to[mm][bl] = o;
+    }
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
+        te[i >> 6][i & 63] = ve[k];
+        to[i >> 6][i & 63] = vo[k];
     }
     __syncthreads();
-    for (int i = tid; i < 64 * MB; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+        const int i = tid + 256 * k;
         const int bl = i / MB, mm = i % MB, b = bz + bl, m = m0 + mm;
         if (b >= nmaps || m >= rp.mt) continue;
         T sc = (T)1;

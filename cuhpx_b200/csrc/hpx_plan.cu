@@ -877,9 +877,7 @@ struct Pipeline {
                 Timer tm(P, st, kStAlmCols);
                 if (amax) {
                     cudaMemsetAsync(amax, 0, sizeof(unsigned) * nb, st);
-                    const int64_t n = (int64_t)P->L * P->M * 2;
-                    const int bx = (int)std::min<int64_t>(64, (n / 4 + 1023) / 1024);
-                    k_rows_maxabs<<<dim3(std::max(bx, 1), nb), 256, 0, st>>>((const float*)alm, n, amax);
+                    k_alm_maxabs<<<dim3((P->L + 7) / 8, nb), 256, 0, st>>>((const float*)alm, P->L, P->M, amax);
                 }
                 dim3 tg((P->M + 31) / 32, P->L + 64);
                 k_alm_to_tc<<<tg, dim3(32, 8), 0, st>>>((const float*)alm, nb, P->L, P->M, TP.Lh, ah, al, amax);

@@ -1026,18 +1026,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // alm[b][l][m] (FP32 complex) -> Ah/Al bf16 [2M][Lh][128]: row i of (m, par) is
 // degree l = m + 2i + par; rows with l >= L (up to L+63) are written as zeros.
 // amax != nullptr: fp16 halves of the values times 2^e(map), e from the map's
-// max |a| (k_rows_maxabs); otherwise bf16 halves.
+// max |a| (k_alm_maxabs); otherwise bf16 halves.
 __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int M, int Lh,
                             uint16_t* __restrict__ ah, uint16_t* __restrict__ al, const unsigned* __restrict__ amax) {
     __shared__ float2 tile[64][33];
+    __shared__ float s_sc[64];
     const int m0 = blockIdx.x * 32, l = blockIdx.y;
+    if (l < m0) return;  // only m <= l is used: nothing to convert in this block
     const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-    for (int i = ty; i < 64; i += 8) {
-        const int m = m0 + tx;
-        float2 v = make_float2(0.f, 0.f);
-        if (i < nmaps && m < M && l < L) v = *(const float2*)(alm + 2 * (((int64_t)i * L + l) * M + m));
-        tile[i][tx] = v;
+    // all loads of the thread are issued before the first shared-memory store
+    float2 vv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = ty + 8 * k, m = m0 + tx;
+        vv[k] = make_float2(0.f, 0.f);
+        if (i < nmaps && m < M && m <= l && l < L) vv[k] = *(const float2*)(alm + 2 * (((int64_t)i * L + l) * M + m));
     }
+    if (amax && ty < 2) {
+        const int b = ty * 32 + tx;
+        s_sc[b] = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? amax[b] : 0u)));
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tile[ty + 8 * k][tx] = vv[k];
     __syncthreads();
     // each warp writes rows for 4 m's: 128 columns as 64 bf16x2 (hi) + 64 (lo)
     for (int mi = ty; mi < 32; mi += 8) {
@@ -1051,7 +1061,7 @@ __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int
             const float2 v = tile[b][mi];
             uint16_t h0, l0, h1, l1;
             if (amax) {
-                const float sc = tc::pow2f(tc::f16_scale_exp(__uint_as_float(b < nmaps ? amax[b] : 0u)));
+                const float sc = s_sc[b];
                 tc::split_f16(v.x * sc, h0, l0);
                 tc::split_f16(v.y * sc, h1, l1);
             } else {
