@@ -491,7 +491,7 @@ def algorithmic(nside, L, M):
         "unfold": 16 * kept_pairs + 8 * kept,  # E and O per (m, ring pair) in, spectra out
         "legendre_forward": 16 * kept_pairs + 8 * tri,  # operand in, order-major rows out (+ table)
         "columns_to_alm": 8 * tri + 8 * L * M,  # rows in, dense alm out
-        "alm_to_columns": 16 * L * M + 8 * tri,  # max scan and read of alm, fp16 hi/lo operand out
+        "alm_to_columns": 8 * tri + 8 * tri,  # alm (m <= l) in once, fp16 hi/lo operand out (the max scan reads it again)
         "legendre_inverse": 8 * tri + 16 * kept_pairs,  # operand in, E and O out (+ table)
     }
     return flops, stage_bytes
@@ -502,14 +502,14 @@ def algorithmic(nside, L, M):
 # table, from one single-pass ncu capture of this script's default workload:
 # stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
 MEASURED_TRAFFIC = {
-    "ring_fft_forward": 3634162688 + 3442558208,
-    "ring_fft_inverse": 3636217856 + 3470151680,
-    "fold": 3222771712 + 3174716160,
-    "legendre_forward": 19722016768 + 1070631680,
-    "columns_to_alm": 1080372224 + 2097201664,
-    "alm_to_columns": (2146283008 + 108544) + (2145484032 + 1078057984),
-    "legendre_inverse": 17335838720 + 3165497088,
-    "unfold": 3224604928 + 3169508608,
+    "ring_fft_forward": 3636297472 + 3445444096,
+    "ring_fft_inverse": 3636335872 + 3471806464,
+    "fold": 3221530112 + 3175441152,
+    "legendre_forward": 19290448128 + 1070319872,
+    "columns_to_alm": 1088316160 + 2099090944,
+    "alm_to_columns": (1089046016 + 121600) + (1088915200 + 1078098688),
+    "legendre_inverse": 17085074432 + 3165567488,
+    "unfold": 3229864192 + 3171027968,
 }
 
 # kernels behind each stage's timer (the mixed path's alm_to_columns is a max

@@ -1084,12 +1084,20 @@ __global__ void k_tc_to_alm(const float* __restrict__ ycols, int nmaps, int L, i
     __shared__ float2 tile[64][33];
     const int m0 = blockIdx.x * 32, l = blockIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int mi = ty; mi < 32; mi += 8) {
-        const int m = m0 + mi;
+    // all loads of the thread are issued before the first shared-memory store
+    float2 vv[4][2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int m = m0 + ty + 8 * k;
         const bool live = m < m_end && m <= l;
         const float2* row = (const float2*)(ycols + ((int64_t)m * L + l) * kTcCols);
-        for (int b = tx; b < 64; b += 32) tile[b][mi] = live ? row[b] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) vv[k][h] = live ? row[tx + 32 * h] : make_float2(0.f, 0.f);
     }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) tile[tx + 32 * h][ty + 8 * k] = vv[k][h];
     __syncthreads();
     const int m = m0 + tx;
     if (m >= m_end) return;
