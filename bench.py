@@ -512,9 +512,13 @@ MEASURED_TRAFFIC = {
     "unfold": 3229864192 + 3171027968,
 }
 
-# kernels behind each stage's timer (the mixed path's alm_to_columns is a max
-# scan plus the conversion when the operand carries a per-map fp16 scale)
+# kernels behind each stage's timer: the ring stages launch the power-of-two
+# rings and the Bluestein rings as two kernels (HEALPix grids have both), and
+# the mixed path's alm_to_columns is a max scan plus the conversion when the
+# operand carries a per-map fp16 scale
 def kernels_in_stage(name, prec):
+    if name.startswith("ring_fft"):
+        return 2
     return 2 if (name == "alm_to_columns" and prec == "f16x3") else 1
 
 

@@ -32,19 +32,49 @@ __device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingP
     return tt + phase_tab_elems(half);
 }
 
-// One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
+// Bluestein rings: the ring's chirp (h entries) and the first half of its chirp
+// spectrum G (P/2 + 1 entries; G_k = G_{P-k}) are staged in shared memory after
+// the phase tables, once per CTA for all its maps; returns the start of the FFT
+// buffers.
 template <typename T>
-__global__ void __launch_bounds__(256, ring_min_ctas<T>())
+__device__ __forceinline__ cplx<T>* ring_bluestein_tables(cplx<T>* smem, const RingPair& rp,
+                                                          const cplx<T>* __restrict__ gtab,
+                                                          const cplx<T>* __restrict__ chirp, const cplx<T>*& Gs,
+                                                          const cplx<T>*& cs) {
+    const int half = (1 << rp.logP) / 2 + 1;
+    cplx<T>* gsm = smem;
+    cplx<T>* csm = smem + half;
+    for (int i = threadIdx.x; i < half; i += blockDim.x) gsm[i] = gtab[rp.gtab_off + i];
+    for (int i = threadIdx.x; i < rp.h; i += blockDim.x) csm[i] = chirp[rp.gtab_off + i];
+    Gs = gsm;
+    cs = csm;
+    return csm + rp.h;
+}
+
+// The ring kernels come in two instantiations launched over two ring lists:
+// power-of-two rings (BLUE = false, 3 CTAs per SM for float) and Bluestein rings
+// (BLUE = true, 2 CTAs per SM with 128 registers and the ring's tables in
+// shared memory).  CTA (blockIdx.x, blockIdx.y) runs ring rings[blockIdx.x]
+// for its group of maps.
+template <typename T, bool BLUE>
+constexpr int ring_kernel_ctas() { return BLUE ? 2 : ring_min_ctas<T>(); }
+
+// One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
+template <typename T, bool BLUE>
+__global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta, T* __restrict__ F, int64_t Ftot, Geom geo,
-               const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
-               unsigned* __restrict__ fmax) {
+               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ gtab,
+               const cplx<T>* __restrict__ chirp, unsigned* __restrict__ fmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
-    const int t = blockIdx.x;
+    const int t = rings[blockIdx.x];
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
     PhaseTab<T> E, tw;
     cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
+    const cplx<T>* Gs = nullptr;
+    const cplx<T>* cs = nullptr;
+    if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);
     __syncthreads();
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
@@ -64,8 +94,8 @@ __global__ void __launch_bounds__(256, ring_min_ctas<T>())
         auto load_next = [&](cplx<T>* dst) {
             if (b + S < b1) ring_load_async(dst, map + (int64_t)(b + S) * np + start, rp.h, lt, tpf);
         };
-        const T mx = ring_forward(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, tw, gtab,
-                                  chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
+        const T mx = ring_forward<BLUE>(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, tw, Gs, cs, E, lt,
+                                        tpf, g, load_next);
         if (fmax) {
             // per-map max |F| (scale of the FP16 operands); a group is whole warps
             float v = (float)mx;
@@ -78,18 +108,21 @@ __global__ void __launch_bounds__(256, ring_min_ctas<T>())
 
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
 // (ref != nullptr: write ref - synthesis)
-template <typename T>
-__global__ void __launch_bounds__(256, ring_min_ctas<T>())
+template <typename T, bool BLUE>
+__global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map, int nmaps, int maps_per_cta, Geom geo,
-               const RingPair* __restrict__ pairs, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
-               const T* __restrict__ ref) {
+               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ gtab,
+               const cplx<T>* __restrict__ chirp, const T* __restrict__ ref) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
-    const int t = blockIdx.x;
+    const int t = rings[blockIdx.x];
     const bool south = t >= NP;
     const RingPair rp = pairs[south ? R - 1 - t : t];
     PhaseTab<T> E, tw;
     cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
+    const cplx<T>* Gs = nullptr;
+    const cplx<T>* cs = nullptr;
+    if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);
     __syncthreads();
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
     const int P = 1 << rp.logP;
@@ -110,8 +143,8 @@ __global__ void __launch_bounds__(256, ring_min_ctas<T>())
         auto load_next = [&](cplx<T>* dst) {
             if (b + S < b1) spec_load_async(dst, spec(b + S), rp.mt, lt, tpf);
         };
-        ring_inverse(cur, other, shift, map + (int64_t)b * np + start, ref ? ref + (int64_t)b * np + start : nullptr,
-                     rp, tw, gtab, chirp + (rp.gtab_off < 0 ? 0 : rp.gtab_off), E, lt, tpf, g, load_next);
+        ring_inverse<BLUE>(cur, other, shift, map + (int64_t)b * np + start,
+                           ref ? ref + (int64_t)b * np + start : nullptr, rp, tw, Gs, cs, E, lt, tpf, g, load_next);
     }
 }
 

@@ -88,6 +88,11 @@ struct hpx_plan_s {
     int nmax = 0;   // max nphi
     std::vector<RingPair> h_pairs;
     RingPair* d_pairs = nullptr;
+    // ring lists of the two ring-kernel instantiations: power-of-two rings, then
+    // Bluestein rings (largest first), as ring indices t
+    int* d_rings = nullptr;
+    int n_rings_pow2 = 0, n_rings_blue = 0;
+    int hblue = 0, pblue = 0;  // largest h and FFT length of the Bluestein rings
     void* d_gtab = nullptr; // cplx<T> Bluestein chirp spectra (natural order)
     void* d_chirp = nullptr; // cplx<T> Bluestein chirps
     int64_t Ftot = 0;        // complex spectrum entries per map over all rings
@@ -105,7 +110,7 @@ struct hpx_plan_s {
     std::vector<int> h_lsmax;
     int n_fwdtiles = 0;
     float wmax = 0.f;            // largest ring weight w_t
-    size_t ring_smem = 0, fwd_smem = 0, inv_smem = 0;
+    size_t ring_smem = 0, blue_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
     // per-kernel event timing (hpx_stats_*)
@@ -136,6 +141,7 @@ struct hpx_plan_s {
         cudaGetDevice(&prev);
         cudaSetDevice(device);
         cudaFree(d_pairs);
+        cudaFree(d_rings);
         cudaFree(d_gtab);
         cudaFree(d_chirp);
         cudaFree(d_lstart);
@@ -223,16 +229,21 @@ int create_typed(hpx_plan_s* P) {
     }
     // shared memory budgets
     P->ring_smem = ring_smem_elems(P->bufP, P->nmax) * sizeof(C);
+    // Bluestein CTAs also hold the ring's chirp and half of its chirp spectrum
+    P->blue_smem = P->n_rings_blue ? (ring_smem_elems(P->bufP, P->nmax) + P->pblue / 2 + 1 + P->hblue) * sizeof(C) : 0;
     P->fwd_smem = fwd_smem_bytes<T>();
     P->inv_smem = inv_smem_bytes<T>(P->L);
     int dev_max = 0;
     HPX_CUDA_TRY(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
-    if ((int)P->ring_smem > dev_max || (int)P->fwd_smem > dev_max || (int)P->inv_smem > dev_max)
+    if ((int)P->ring_smem > dev_max || (int)P->blue_smem > dev_max || (int)P->fwd_smem > dev_max ||
+        (int)P->inv_smem > dev_max)
         return set_err(HPX_ERR_UNSUPPORTED, "nside/lmax too large for the shared-memory kernels of this precision");
     // The attribute is per function, not per plan: always raise it to the device
     // maximum so that a plan needing less never lowers it under another plan.
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     return HPX_OK;
@@ -620,6 +631,26 @@ int plan_build(hpx_plan_s* P) {
 
     HPX_CUDA_TRY(cudaMalloc(&P->d_pairs, sizeof(RingPair) * P->NP));
     HPX_CUDA_TRY(cudaMemcpy(P->d_pairs, P->h_pairs.data(), sizeof(RingPair) * P->NP, cudaMemcpyHostToDevice));
+    {
+        std::vector<int> pw, bl;
+        auto pair_of = [&](int t) -> const RingPair& { return P->h_pairs[t < P->NP ? t : P->R - 1 - t]; };
+        for (int t = 0; t < P->R; ++t) {
+            const RingPair& rp = pair_of(t);
+            if (rp.logh >= 0) {
+                pw.push_back(t);
+            } else {
+                bl.push_back(t);
+                P->hblue = std::max(P->hblue, rp.h);
+                P->pblue = std::max(P->pblue, 1 << rp.logP);
+            }
+        }
+        std::stable_sort(bl.begin(), bl.end(), [&](int a, int b) { return pair_of(a).h > pair_of(b).h; });
+        P->n_rings_pow2 = (int)pw.size();
+        P->n_rings_blue = (int)bl.size();
+        pw.insert(pw.end(), bl.begin(), bl.end());
+        HPX_CUDA_TRY(cudaMalloc(&P->d_rings, sizeof(int) * pw.size()));
+        HPX_CUDA_TRY(cudaMemcpy(P->d_rings, pw.data(), sizeof(int) * pw.size(), cudaMemcpyHostToDevice));
+    }
 
     // ---- Legendre start values
     std::vector<double> logc(P->M);
@@ -811,9 +842,15 @@ struct Pipeline {
         {
             Timer tm(P, st, kStRingFwd);
             if (fmax) cudaMemsetAsync(fmax, 0, sizeof(unsigned) * nb, st);
-            dim3 grid(P->R, (nb + g - 1) / g);
-            k_ring_fwd<T><<<grid, 256, P->ring_smem, st>>>(map, nb, g, F, P->Ftot, P->geo, P->d_pairs,
-                                                          (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, fmax);
+            const unsigned nbk = (nb + g - 1) / g;
+            const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
+            const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
+            if (P->n_rings_pow2)
+                k_ring_fwd<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, st>>>(
+                    map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, gt, ch, fmax);
+            if (P->n_rings_blue)
+                k_ring_fwd<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, st>>>(
+                    map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, fmax);
         }
         Timer tm(P, st, kStFold);
         // |c (F_t +- F_t')| <= 2 max|c| max|F|: c = w_t, or c_m <= 2 for the adjoint
@@ -831,9 +868,15 @@ struct Pipeline {
         }
         const int g = maps_per_cta_ring();
         Timer tm(P, st, kStRingInv);
-        dim3 grid(P->R, (nb + g - 1) / g);
-        k_ring_inv<T><<<grid, 256, P->ring_smem, st>>>(F, P->Ftot, map, nb, g, P->geo, P->d_pairs,
-                                                      (const cplx<T>*)P->d_gtab, (const cplx<T>*)P->d_chirp, ref);
+        const unsigned nbk = (nb + g - 1) / g;
+        const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
+        const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
+        if (P->n_rings_pow2)
+            k_ring_inv<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, st>>>(
+                F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, gt, ch, ref);
+        if (P->n_rings_blue)
+            k_ring_inv<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, st>>>(
+                F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, ref);
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();

@@ -412,9 +412,12 @@ __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW&
 // fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).  ZIN / HOUT
 // as for fft_pass_ct (the generic passes ignore them: they transform and store
 // everything, which is also correct).
+// (tw, pre and post by value: this function may not be inlined, and a
+// reference would make every twiddle lookup reload the table's pointers from
+// the stack)
 template <typename T, bool INV, bool ZIN = false, bool HOUT = false, typename TW, typename Pre, typename Post>
-__device__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const TW& tw, int lt, int tpf, int g, Pre pre,
-                             Post post) {
+__device__ __forceinline__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const TW tw, int lt, int tpf, int g,
+                                             Pre pre, Post post) {
     if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
     switch (logP) {
         case 1: return fft_ct<T, INV, 1, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
@@ -445,41 +448,43 @@ __device__ void load_twiddles(cplx<T>* twP, int logP, const cplx<T>* __restrict_
 
 // Complex DFT of length h of buf (natural order, h entries written by this
 // group), forward (e^-) or inverse (e^+); returns the buffer with Z in natural order.
-template <typename T, typename TW>
-__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const TW& tw,
-                             const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp, bool inv, int lt,
-                             int tpf, int g) {
+template <bool BLUE, typename T, typename TW>
+__device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const TW tw, const cplx<T>* __restrict__ G,
+                             const cplx<T>* __restrict__ chirp, bool inv, int lt, int tpf, int g) {
     group_sync(tpf, g);
     IdentityMap id;
-    if (rp.logh >= 0) {
+    if constexpr (!BLUE) {
+        // power-of-two ring
         if (rp.logh == 0) return buf;
         return inv ? fft_ring<T, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
                    : fft_ring<T, false>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id);
+    } else {
+        // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
+        // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
+        // (scaled by 1/P); the inverse transform is conj(DFT(conj z)).  The chirp
+        // products ride on the first loads and the last stores of the two FFTs.
+        // chirp[0..h) and G[0..P/2] are the ring's tables in shared memory (G is
+        // symmetric, G_k = G_{P-k}).
+        const int h = rp.h, P = 1 << rp.logP;
+        // captures by value: the passes may run in a called (not inlined) function,
+        // where a captured reference would be a load from the stack per element
+        auto pre = [h, inv, chirp](int j, cplx<T> a) {
+            if (j >= h) return cplx<T>{(T)0, (T)0};
+            if (inv) a.im = -a.im;
+            return cmul(a, chirp[j]);
+        };
+        auto mulG = [G, P](int k, cplx<T> a) { return cmul(a, G[2 * k <= P ? k : P - k]); };
+        auto postc = [h, inv, chirp](int k, cplx<T> a) {
+            if (k >= h) return a;
+            cplx<T> v = cmul(a, chirp[k]);
+            if (inv) v.im = -v.im;
+            return v;
+        };
+        // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
+        cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
+        cplx<T>* o = (r == buf) ? buf2 : buf;
+        return fft_ring<T, true, false, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
     }
-    // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
-    // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
-    // (scaled by 1/P); the inverse transform is conj(DFT(conj z)).  The chirp
-    // products ride on the first loads and the last stores of the two FFTs.
-    const int h = rp.h;
-    const cplx<T>* G = gtab + rp.gtab_off;
-    // captures by value: the passes may run in a called (not inlined) function,
-    // where a captured reference would be a load from the stack per element
-    auto pre = [h, inv, chirp](int j, cplx<T> a) {
-        if (j >= h) return cplx<T>{(T)0, (T)0};
-        if (inv) a.im = -a.im;
-        return cmul(a, chirp[j]);
-    };
-    auto mulG = [G](int k, cplx<T> a) { return cmul(a, G[k]); };
-    auto postc = [h, inv, chirp](int k, cplx<T> a) {
-        if (k >= h) return a;
-        cplx<T> v = cmul(a, chirp[k]);
-        if (inv) v.im = -v.im;
-        return v;
-    };
-    // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
-    cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
-    cplx<T>* o = (r == buf) ? buf2 : buf;
-    return fft_ring<T, true, false, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
 }
 
 // One complex element (8 or 16 bytes) global -> shared, asynchronously.
@@ -510,14 +515,14 @@ __device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg,
 // free receives the next map's ring (load_next, asynchronous) while this map's
 // spectrum is formed and stored.  On return cur holds the next input.
 // Returns the largest |re|, |im| this thread wrote.
-template <typename T, typename Next>
+template <bool BLUE, typename T, typename Next>
 __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ F, const RingPair& rp,
                           const PhaseTab<T>& tw, const cplx<T>* __restrict__ gtab,
                           const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g,
                           Next load_next) {
     const int h = rp.h;
     cp_async_wait<0>();
-    cplx<T>* Z = ring_dft(cur, other, rp, tw, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
+    cplx<T>* Z = ring_dft<BLUE>(cur, other, rp, tw, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (Z == cur) ? other : cur;
     load_next(freeb);
     T mx = (T)0;
@@ -560,7 +565,7 @@ __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restri
 // DFT runs there, and the buffer it leaves free receives the next map's
 // spectrum (load_next) while this ring is stored.  On return cur holds the
 // next input.  ref != nullptr: write ref - x (Jacobi residual).
-template <typename T, typename Next>
+template <bool BLUE, typename T, typename Next>
 __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ x,
                              const T* __restrict__ ref, const RingPair& rp, const PhaseTab<T>& tw,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
@@ -589,7 +594,7 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
         buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
         if (k != 0 && kb != k) buf[padi(kb)] = {sum.re + r.im, r.re - sum.im};
     }
-    cplx<T>* z = ring_dft(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
+    cplx<T>* z = ring_dft<BLUE>(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
     load_next(freeb);
     for (int j = lt; j < h; j += tpf) {
