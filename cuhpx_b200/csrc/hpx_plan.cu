@@ -93,6 +93,12 @@ struct hpx_plan_s {
     int* d_rings = nullptr;
     int n_rings_pow2 = 0, n_rings_blue = 0;
     int hblue = 0, pblue = 0;  // largest h and FFT length of the Bluestein rings
+    // auxiliary stream and fork/join events: the two ring launches of a
+    // transform overlap (the power-of-two rings run on aux); the mutex keeps
+    // the record/wait pairs of concurrent callers of one plan apart
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    mutable std::mutex fork_mu;
     void* d_gtab = nullptr; // cplx<T> Bluestein chirp spectra (natural order)
     void* d_chirp = nullptr; // cplx<T> Bluestein chirps
     int64_t Ftot = 0;        // complex spectrum entries per map over all rings
@@ -142,6 +148,9 @@ struct hpx_plan_s {
         cudaSetDevice(device);
         cudaFree(d_pairs);
         cudaFree(d_rings);
+        if (aux) cudaStreamDestroy(aux);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         cudaFree(d_gtab);
         cudaFree(d_chirp);
         cudaFree(d_lstart);
@@ -240,6 +249,9 @@ int create_typed(hpx_plan_s* P) {
         return set_err(HPX_ERR_UNSUPPORTED, "nside/lmax too large for the shared-memory kernels of this precision");
     // The attribute is per function, not per plan: always raise it to the device
     // maximum so that a plan needing less never lowers it under another plan.
+    HPX_CUDA_TRY(cudaStreamCreateWithFlags(&P->aux, cudaStreamNonBlocking));
+    HPX_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
+    HPX_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
@@ -836,6 +848,28 @@ struct Pipeline {
 
     int maps_per_cta_ring() const { return 8; }
 
+    // The power-of-two rings on the plan's auxiliary stream and the Bluestein
+    // rings on st, forked and joined by events (valid under stream capture), so
+    // that the two launches and their tails overlap.
+    template <typename Pow2, typename Blue>
+    void ring_launches(Pow2 pow2, Blue blue) {
+        if (P->n_rings_pow2 && P->n_rings_blue) {
+            std::lock_guard<std::mutex> lk(P->fork_mu);
+            cudaError_t e = cudaEventRecord(P->ev_fork, st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(P->aux, P->ev_fork, 0);
+            if (e == cudaSuccess) {
+                pow2(P->aux);
+                blue(st);
+                e = cudaEventRecord(P->ev_join, P->aux);
+            }
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, P->ev_join, 0);
+            if (e != cudaSuccess) rc = set_err(HPX_ERR_CUDA, std::string("ring stream fork/join: ") + cudaGetErrorString(e));
+            return;
+        }
+        if (P->n_rings_pow2) pow2(st);
+        if (P->n_rings_blue) blue(st);
+    }
+
     // map -> ring spectra F -> folded Legendre operand (spec, or bf16 hi/lo)
     void ring_fwd(const T* map, int nb, int adjoint) {
         const int g = maps_per_cta_ring();
@@ -845,12 +879,15 @@ struct Pipeline {
             const unsigned nbk = (nb + g - 1) / g;
             const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
             const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
-            if (P->n_rings_pow2)
-                k_ring_fwd<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, st>>>(
-                    map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, gt, ch, fmax);
-            if (P->n_rings_blue)
-                k_ring_fwd<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, st>>>(
-                    map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, fmax);
+            ring_launches(
+                [&](cudaStream_t s) {
+                    k_ring_fwd<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
+                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, gt, ch, fmax);
+                },
+                [&](cudaStream_t s) {
+                    k_ring_fwd<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
+                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, fmax);
+                });
         }
         Timer tm(P, st, kStFold);
         // |c (F_t +- F_t')| <= 2 max|c| max|F|: c = w_t, or c_m <= 2 for the adjoint
@@ -871,12 +908,15 @@ struct Pipeline {
         const unsigned nbk = (nb + g - 1) / g;
         const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
         const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
-        if (P->n_rings_pow2)
-            k_ring_inv<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, st>>>(
-                F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, gt, ch, ref);
-        if (P->n_rings_blue)
-            k_ring_inv<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, st>>>(
-                F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, ref);
+        ring_launches(
+            [&](cudaStream_t s) {
+                k_ring_inv<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
+                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, gt, ch, ref);
+            },
+            [&](cudaStream_t s) {
+                k_ring_inv<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
+                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, ref);
+            });
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
         const int C = P->cols();
