@@ -502,14 +502,14 @@ def algorithmic(nside, L, M):
 # table, from one single-pass ncu capture of this script's default workload:
 # stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
 MEASURED_TRAFFIC = {
-    "ring_fft_forward": 3636297472 + 3445444096,
-    "ring_fft_inverse": 3636335872 + 3471806464,
-    "fold": 3221530112 + 3175441152,
-    "legendre_forward": 19290448128 + 1070319872,
-    "columns_to_alm": 1088316160 + 2099090944,
-    "alm_to_columns": (1089046016 + 121600) + (1088915200 + 1078098688),
-    "legendre_inverse": 17085074432 + 3165567488,
-    "unfold": 3229864192 + 3171027968,
+    "ring_fft_forward": (2152408576 + 2101460992) + (1231005440 + 1028252416),
+    "ring_fft_inverse": (2151525888 + 2112886016) + (1232021248 + 1027889920),
+    "fold": 3221534208 + 3172663296,
+    "legendre_forward": 19294675200 + 1070779392,
+    "columns_to_alm": 1088915456 + 2099540736,
+    "alm_to_columns": (1089042432 + 132096) + (1088926464 + 1077800960),
+    "legendre_inverse": 17085071360 + 3165193984,
+    "unfold": 3230080000 + 3172550656,
 }
 
 # kernels behind each stage's timer: the ring stages launch the power-of-two
