@@ -38,7 +38,9 @@ def hpx(cuda):
     return cuhpx_b200
 
 
-CASES = [(16, 32, None, None), (17, 32, 12, 10), (33, 64, None, None), (64, 128, 48, 40), (8, 16, 12, 12)]
+# nlon = 36 and 90 give non-power-of-two rings (Bluestein kernel only; h = 45 is odd)
+CASES = [(16, 32, None, None), (17, 32, 12, 10), (33, 64, None, None), (64, 128, 48, 40), (8, 16, 12, 12),
+         (18, 36, None, None), (45, 90, 30, 28)]
 
 
 @pytest.mark.parametrize("grid", GRIDS)
