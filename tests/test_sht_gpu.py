@@ -188,6 +188,38 @@ def test_deterministic(hpx, cuda):
     assert torch.equal(a1, a2)
 
 
+def test_one_plan_two_streams_two_threads(hpx, cuda):
+    """Two host threads drive the same plan on two streams at once: each call's
+    ring FFT forks onto the plan's own stream and joins back, and the results
+    equal those of serial calls."""
+    import threading
+
+    rng = np.random.default_rng(11)
+    nside, L = 64, 127
+    fs = [torch.from_numpy(rng.standard_normal((8, 12 * nside * nside))).float().to(cuda) for _ in range(2)]
+    sht = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision="f16x3", refine_iters=0)
+    isht = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision="f16x3")
+    ref = [isht(sht(f)) for f in fs]
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(cuda) for _ in range(2)]
+    out = [[None] * 6, [None] * 6]
+
+    def work(i):
+        with torch.cuda.stream(streams[i]):
+            for r in range(6):
+                out[i][r] = isht(sht(fs[i]))
+
+    ths = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    torch.cuda.synchronize()
+    for i in range(2):
+        for r in range(6):
+            assert torch.equal(out[i][r], ref[i])
+
+
 # ------------------------------------------------------------------ adjoints
 def _dot_alm(a, b):
     return float(torch.sum(a.real * b.real + a.imag * b.imag))
