@@ -306,13 +306,19 @@ def run_gpu(args):
     # end to end through the public modules with host buffers
     e2e = None
     if not args.no_e2e:
-        ms_e, ksteps = e2e_pipelined(torch, sht, isht, f, dev, args.steps, args.warmup, dist)
+        # the pipeline's fill (first upload) and drain (last download) do not
+        # overlap anything: at least 30 steps amortise them (about 2 s).  Cached
+        # blocks of the earlier runs are returned first, so that the pipeline's
+        # buffers do not have to displace them inside the timed region.
+        torch.cuda.empty_cache()
+        ms_e, ksteps = e2e_pipelined(torch, sht, isht, f, dev, max(args.steps, 30), args.warmup, dist)
         nb = f.numel() * f.element_size()
         e2e = {
             "value": world * B * ksteps / (ms_e / 1000.0),
             "unit": "maps/s",
             "h2d_bytes_per_step": nb,
             "d2h_bytes_per_step": nb,
+            "steps": ksteps,
             "pipeline": "every step copies its 64 maps host->device (pinned), runs SHT+iSHT through "
             "SHTCUDA/iSHTCUDA and copies the maps back; upload of step i+1 and download of step i-1 "
             "overlap step i on three streams",
@@ -421,6 +427,12 @@ def e2e_pipelined(torch, sht, isht, f, dev, steps, warmup, dist):
                     s_in.wait_event(ev_c[k])  # step i-2 has finished reading din[k]
                 din[k].copy_(hin[k], non_blocking=True)
                 ev_in[k].record(s_in)
+            if ys[k] is not None:
+                # step i-2's result is released only once its download is done, so that the
+                # allocator hands its block to the compute stream again (no record_stream,
+                # whose deferred frees make the cache grow with every step)
+                ev_out[k].synchronize()
+                ys[k] = None
             with torch.cuda.stream(s_c):
                 s_c.wait_event(ev_in[k])
                 with torch.no_grad():
@@ -428,7 +440,6 @@ def e2e_pipelined(torch, sht, isht, f, dev, steps, warmup, dist):
                 ev_c[k].record(s_c)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_c[k])
-                ys[k].record_stream(s_out)
                 hout[k].copy_(ys[k], non_blocking=True)
                 ev_out[k].record(s_out)
 
