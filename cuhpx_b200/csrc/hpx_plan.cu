@@ -277,7 +277,18 @@ int schedule_tiles(const std::vector<int2>& tiles, const std::vector<double>& co
     const int nc = std::max(1, std::min(nsm, n));
     std::vector<int> idx(n);
     for (int i = 0; i < n; ++i) idx[i] = i;
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    // sort by the total cost of the tile's order: the tiles of one order (m-major
+    // input, stable sort) stay together, are dealt to neighbouring CTAs in the
+    // same rounds and share the order's data operand in L2
+    std::vector<double> mcost(n);
+    for (int i = 0; i < n;) {
+        int j = i;
+        double c = 0.0;
+        while (j < n && tiles[j].x == tiles[i].x) c += cost[j++];
+        for (int k = i; k < j; ++k) mcost[k] = c;
+        i = j;
+    }
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return mcost[a] > mcost[b]; });
     std::vector<std::vector<int>> per(nc);
     for (int k = 0; k < n; ++k) {
         const int round = k / nc, pos = k % nc;
@@ -356,11 +367,52 @@ int tc_create(hpx_plan_s* P) {
     T.Lh = (P->L + 65) / 2;
     const int rc = tc_table_create(P);
     if (rc != HPX_OK) return rc;
+    // With the table: first nonzero degree of every (m, ring), so that each tile
+    // starts past its all-zero chunks (tile words: fwd_tile_c0 / inv_tile_c0).
+    std::vector<int> fnz;
+    if (T.table) {
+        int* d_fnz = nullptr;
+        HPX_CUDA_TRY(cudaMalloc(&d_fnz, sizeof(int) * (size_t)T.m_tc_end * P->NP));
+        k_table_first_nz<<<dim3(P->NP, T.m_tc_end), 64>>>(T.d_table, P->NP, T.Lt, d_fnz);
+        fnz.resize((size_t)T.m_tc_end * P->NP);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(fnz.data(), d_fnz, sizeof(int) * fnz.size(), cudaMemcpyDeviceToHost);
+        cudaFree(d_fnz);
+        if (e != cudaSuccess) return set_err(HPX_ERR_CUDA, std::string("table scan: ") + cudaGetErrorString(e));
+    }
     std::vector<int2> ft, it;
+    std::vector<int> fch, ich;  // chunks each tile runs
     for (int m = 0; m < T.m_tc_end; ++m) {
-        for (int j = 0; j < (P->L - m + kTcFwdDeg - 1) / kTcFwdDeg; ++j) ft.push_back(make_int2(m, j));
-        const int K = P->NP - P->geo.first_ring(m);
-        for (int rb = 0; rb < K; rb += kTcInvRings) it.push_back(make_int2(m, rb));
+        const int t0 = P->geo.first_ring(m);
+        const int nchF = (P->NP - t0 + kFRingS<true> - 1) / kFRingS<true>;
+        const int nchI = (P->L - m + kTcDegChunk - 1) / kTcDegChunk;
+        const int* fz = T.table ? fnz.data() + (size_t)m * P->NP : nullptr;
+        for (int j = 0; j < (P->L - m + kTcFwdDeg - 1) / kTcFwdDeg; ++j) {
+            int c0 = 0;
+            if (T.table) {
+                while (c0 < nchF - 1) {
+                    bool nz = false;
+                    for (int p = t0 + c0 * kFRingS<true>; p < std::min(P->NP, t0 + (c0 + 1) * kFRingS<true>); ++p)
+                        nz = nz || fz[p] < (j + 1) * kTcFwdDeg;
+                    if (nz) break;
+                    ++c0;
+                }
+                fch.push_back(nchF - c0);
+            } else {
+                fch.push_back((P->NP - t0 + kFRing - 1) / kFRing);
+            }
+            ft.push_back(make_int2(m, j | (c0 << 8)));
+        }
+        for (int rb = 0; rb < P->NP - t0; rb += kTcInvRings) {
+            int c0 = 0;
+            if (T.table) {
+                int dmin = 1 << 30;
+                for (int p = t0 + rb; p < std::min(P->NP, t0 + rb + kTcInvRings); ++p) dmin = std::min(dmin, fz[p]);
+                c0 = std::min(dmin / kTcDegChunk, std::max(nchI - 1, 0));
+            }
+            ich.push_back(nchI - c0);
+            it.push_back(make_int2(m, rb | (c0 << 16)));
+        }
     }
     T.n_fwd_tiles = (int)ft.size();
     T.n_inv_tiles = (int)it.size();
@@ -370,15 +422,20 @@ int tc_create(hpx_plan_s* P) {
     // producers' slower start-injecting recurrence (about twice the time);
     // with it every chunk costs the same, and the tiles of one order sort
     // together, run at the same time and share its data operand in L2.
+    // (with the table a chunk holds 32 rings, twice the producer-fed 16: its
+    // cost counts double)
     const double kSlow = T.table ? 1.0 : 2.0, kTileFixed = 7.0;
     std::vector<double> fc, ic;
-    for (const int2& t : ft) {
-        const int nch = (P->NP - P->geo.first_ring(t.x) + kFRing - 1) / kFRing;
-        fc.push_back(nch * (t.x + t.y * kTcFwdDeg < P->h_lsmax[t.x] ? kSlow : 1.0) + kTileFixed);
+    for (size_t k = 0; k < ft.size(); ++k) {
+        const int2& t = ft[k];
+        const double w = T.table ? 2.0 : (t.x + fwd_tile_jb(t.y) * kTcFwdDeg < P->h_lsmax[t.x] ? kSlow : 1.0);
+        fc.push_back(fch[k] * w + kTileFixed);
     }
-    for (const int2& t : it) {
+    for (size_t k = 0; k < it.size(); ++k) {
+        const int2& t = it[k];
         double c = kTileFixed;
-        for (int l0 = t.x; l0 < P->L; l0 += kTcDegChunk) c += l0 < P->h_lsmax[t.x] ? kSlow : 1.0;
+        const int nchI = (P->L - t.x + kTcDegChunk - 1) / kTcDegChunk;
+        for (int ci = nchI - ich[k]; ci < nchI; ++ci) c += t.x + ci * kTcDegChunk < P->h_lsmax[t.x] ? kSlow : 1.0;
         ic.push_back(c);
     }
     std::vector<int2> order;

@@ -82,6 +82,17 @@ constexpr int kEpiStride = 20;
 constexpr int kEpiStageFloats = 32 * kEpiStride;  // per warp
 constexpr int kEpiStageBytes = 8 * kEpiStageFloats * 4;
 
+// Tile words.  Analysis tile (m, y): degree tile jb = y & 255 and, with the
+// resident table, the first pipeline chunk c0 = y >> 8 whose rings hold a
+// nonzero table entry for the tile's degrees (the chunks before it are all
+// zeros -- polar rings below the turning point -- and are skipped, which
+// leaves the sums bit for bit unchanged).  Synthesis tile (m, y): ring block
+// rb = y & 0xffff and first degree chunk c0 = y >> 16, likewise.
+__host__ __device__ constexpr int fwd_tile_jb(int y) { return y & 255; }
+__host__ __device__ constexpr int fwd_tile_c0(int y) { return y >> 8; }
+__host__ __device__ constexpr int inv_tile_rb(int y) { return y & 0xffff; }
+__host__ __device__ constexpr int inv_tile_c0(int y) { return y >> 16; }
+
 // analysis: 6 stages of 16 rings (32 KB: A 4 x 4 KB, B 4 x 4 KB)
 constexpr int kFStages = 6;
 constexpr int kFRing = 16;
@@ -404,6 +415,30 @@ __global__ void __launch_bounds__(128) k_legendre_table(int m_end, int L, int Lp
     }
 }
 
+// First nonzero entry of each (m, ring) of the table: out[m * NP + p] = the
+// smallest d = l - m whose hi half is nonzero in either parity, or 1 << 30.
+// A zero hi half means a zero lo half too (|Pbar| below the smallest
+// subnormal of the half type).  Block of 64 threads per (ring, m): warp w
+// scans parity w.
+__global__ void __launch_bounds__(64) k_table_first_nz(const uint16_t* __restrict__ tab, int NP, int Lt,
+                                                       int* __restrict__ out) {
+    const int p = blockIdx.x, m = blockIdx.y, par = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint16_t* row = tab + ((((int64_t)m * 2 + par) * 2 + 0) * NP + p) * Lt;
+    int first = 1 << 30;
+    for (int i0 = 0; i0 < Lt; i0 += 32) {
+        const int i = i0 + lane;
+        const unsigned nz = __ballot_sync(0xffffffffu, i < Lt && row[i] != 0);
+        if (nz) {
+            first = 2 * (i0 + __ffs(nz) - 1) + par;
+            break;
+        }
+    }
+    __shared__ int s_first[2];
+    if (lane == 0) s_first[par] = first;
+    __syncthreads();
+    if (threadIdx.x == 0) out[(int64_t)m * NP + p] = min(s_first[0], s_first[1]);
+}
+
 // ================================================================== analysis
 // Xh/Xl: bf16 [2M][NP][128] (hi and lo of S (par 0) and D (par 1)) via tensor maps.
 // Tile (m, 256 degrees); pipeline chunk = 16 rings.  Stage layout:
@@ -449,10 +484,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (TAB) tc::tma_prefetch_desc(&tab_map);
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
-                const int m = tiles[t].x, jb = tiles[t].y;
+                const int m = tiles[t].x, jb = fwd_tile_jb(tiles[t].y), c0 = fwd_tile_c0(tiles[t].y);
                 const int t0 = geo.first_ring(m);
                 const int nch = nchunks(m);
-                for (int c = 0; c < nch; ++c, ++it) {
+                for (int c = c0; c < nch; ++c, ++it) {
                     const int s = it % NS;
                     if (!tc::mbar_wait(&sh->empty[s], ((it / NS) & 1) ^ 1, err, 11)) goto tma_done;
                     unsigned char* st = stages + s * SB + SB / 2;
@@ -488,13 +523,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, true, true) : tc::idesc_bf16(128, kTcCols, true, true);
             int it = 0, tcount = 0;
             for (int t = t_begin; t < t_end; ++t, ++tcount) {
-                const int m = tiles[t].x;
+                const int m = tiles[t].x, c0 = fwd_tile_c0(tiles[t].y);
                 const int nch = nchunks(m);
                 TCP_T0(w2);
                 if (!tc::mbar_wait(&sh->acc_empty[0], (tcount & 1) ^ 1, err, 12)) break;
                 TCP_ADD(0, 2, w2);
                 tc::tc_fence_after();
-                for (int c = 0; c < nch; ++c, ++it) {
+                for (int c = c0; c < nch; ++c, ++it) {
                     const int s = it % NS;
                     const uint32_t ph = (it / NS) & 1;
                     TCP_T0(w0);
@@ -517,7 +552,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const uint64_t al = tc::smem_desc_sw128(sa + (par * 2 + 1) * (SB / 8) + ko, SB / 16, 1024);
                             const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * (SB / 8) + ko, SB / 16, 1024);
                             const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * (SB / 8) + ko, SB / 16, 1024);
-                            const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+                            const uint32_t acc = (c > c0 || ks > 0) ? 1u : 0u;
                             tc::mma_bf16(dm, ah, bh, idesc, acc);
                             tc::mma_bf16(dc, ah, bl, idesc, acc);
                             tc::mma_bf16(dc, al, bh, idesc, 1u);
@@ -543,7 +578,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int par_hi = kEpiWarps<TAB> == 8 ? par_lo + 1 : 2;
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
-            const int m = tiles[t].x, jb = tiles[t].y;
+            const int m = tiles[t].x, jb = fwd_tile_jb(tiles[t].y);
             const int l0 = m + jb * kTcFwdDeg;
             TCP_T0(e0);
             if (!tc::mbar_wait_warp(&sh->acc_full[0], tcount & 1, err, 15)) break;
@@ -603,7 +638,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (t < t_end) {
                 const int2 tt = tiles[t];
                 m = tt.x;
-                jb = tt.y;
+                jb = fwd_tile_jb(tt.y);
                 t0 = geo.first_ring(m);
                 nch = nchunks(m);
             }
@@ -758,10 +793,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (TAB) tc::tma_prefetch_desc(&tab_map);
             int it = 0;
             for (int t = t_begin; t < t_end; ++t) {
-                const int m = tiles[t].x, rb = tiles[t].y;
+                const int m = tiles[t].x, rb = inv_tile_rb(tiles[t].y), c0 = inv_tile_c0(tiles[t].y);
                 const int t0 = geo.first_ring(m);
                 const int nch = nchunks(m);
-                for (int c = 0; c < nch; ++c, ++it) {
+                for (int c = c0; c < nch; ++c, ++it) {
                     const int s = it % kIStages;
                     if (!tc::mbar_wait(&sh->empty[s], ((it / kIStages) & 1) ^ 1, err, 21)) goto tma_done;
                     unsigned char* st = stages + s * kIStageBytes + 32768;
@@ -794,13 +829,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint32_t idesc = F16 ? tc::idesc_f16(128, kTcCols, false, true) : tc::idesc_bf16(128, kTcCols, false, true);
             int it = 0, tcount = 0;
             for (int t = t_begin; t < t_end; ++t, ++tcount) {
-                const int m = tiles[t].x;
+                const int m = tiles[t].x, c0 = inv_tile_c0(tiles[t].y);
                 const int nch = nchunks(m);
                 TCP_T0(w2);
                 if (!tc::mbar_wait(&sh->acc_empty[0], (tcount & 1) ^ 1, err, 22)) break;
                 TCP_ADD(1, 2, w2);
                 tc::tc_fence_after();
-                for (int c = 0; c < nch; ++c, ++it) {
+                for (int c = c0; c < nch; ++c, ++it) {
                     const int s = it % kIStages;
                     const uint32_t ph = (it / kIStages) & 1;
                     TCP_T0(w0);
@@ -821,7 +856,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const uint64_t al = tc::smem_desc_kmajor_sw64(sa + (par * 2 + 1) * 8192 + ks * 32, 512);
                             const uint64_t bh = tc::smem_desc_sw128(sb + (par * 2 + 0) * 8192 + ks * 2048, 4096, 1024);
                             const uint64_t bl = tc::smem_desc_sw128(sb + (par * 2 + 1) * 8192 + ks * 2048, 4096, 1024);
-                            const uint32_t acc = (c > 0 || ks > 0) ? 1u : 0u;
+                            const uint32_t acc = (c > c0 || ks > 0) ? 1u : 0u;
                             tc::mma_bf16(dm, ah, bh, idesc, acc);
                             tc::mma_bf16(dc, ah, bl, idesc, acc);
                             tc::mma_bf16(dc, al, bh, idesc, 1u);
@@ -844,7 +879,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int par_hi = kEpiWarps<TAB> == 8 ? par_lo + 1 : 2;
         int tcount = 0;
         for (int t = t_begin; t < t_end; ++t, ++tcount) {
-            const int m = tiles[t].x, rb = tiles[t].y;
+            const int m = tiles[t].x, rb = inv_tile_rb(tiles[t].y);
             const int t0 = geo.first_ring(m);
             const int rr = rb + ew * 32 + lane;
             const int p = t0 + rr;
@@ -915,7 +950,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (t < t_end) {
                 const int2 tt = tiles[t];
                 m = tt.x;
-                rb = tt.y;
+                rb = inv_tile_rb(tt.y);
                 t0 = geo.first_ring(m);
                 nch = nchunks(m);
             }
