@@ -288,7 +288,7 @@ def run_gpu(args):
     launches_per_step = sum(v[0] * kernels_in_stage(k, prec) for k, v in stats.items()) / args.steps
 
     # roofline of the dominant kernel
-    roof = roofline(stats, args, prec, refine, nside, L, B, plan.table_bytes > 0)
+    roof = roofline(stats, args, prec, refine, nside, L, B, plan.table_bytes > 0, plan.table_stream_bytes)
 
     # plain FP32 comparison (the target is >= 2x this on the same GPU)
     plain = None
@@ -541,10 +541,12 @@ def load_peaks():
     return 6650.0, 1590.0, "fallback (no MEASURED_PEAKS.json): 6650 GB/s and 1590 TFLOP/s, an earlier measurement on this pool"
 
 
-def roofline(stats, args, prec, refine, nside, L, B, table):
+def roofline(stats, args, prec, refine, nside, L, B, table, stream=(0, 0)):
     """Roofline of every timed stage and of the dominant one (largest time).
-    Table-driven contractions stream their operands and the resident table and
-    are HBM-bound; their tensor-core rate is reported beside it."""
+    Table-driven contractions stream their operands and the part of the
+    resident table that holds nonzero entries (`stream`: bytes per pass in each
+    direction, from the plan) and are HBM-bound; their executed tensor-core
+    rate is reported beside it."""
     hbm, bf16, source = load_peaks()
     flops_map, stage_bytes = algorithmic(nside, L, L)
     chunk = min(B, 64)
@@ -565,9 +567,13 @@ def roofline(stats, args, prec, refine, nside, L, B, table):
         else:
             byts = stage_bytes.get(name, 0) * chunk
             if name.startswith("legendre"):
-                byts += flops_map
-                e["tensor_tflops"] = 3 * flops_map * chunk / (ms * 1e-3) / 1e12
+                tb = stream[0] if name == "legendre_forward" else stream[1]
+                tb = tb or flops_map
+                byts += tb
+                # executed: 3 products over the table blocks streamed
+                e["tensor_tflops"] = 3 * tb * chunk / (ms * 1e-3) / 1e12
                 e["tensor_frac"] = e["tensor_tflops"] / bf16
+                e["table_bytes"] = tb
             e.update(bound="hbm", achieved=byts / (ms * 1e-3) / 1e9, peak=hbm, unit="GB/s", algorithmic_bytes=byts)
         e["frac"] = e["achieved"] / e["peak"]
         e["traffic"] = MEASURED_TRAFFIC.get(name) if measured else None

@@ -416,6 +416,11 @@ int tc_create(hpx_plan_s* P) {
     }
     T.n_fwd_tiles = (int)ft.size();
     T.n_inv_tiles = (int)it.size();
+    if (T.table) {
+        // table part of a pipeline stage: 32 KB in both directions
+        for (int c : fch) T.stream_fwd += (size_t)c * (kFStageBytesS<true> / 2);
+        for (int c : ich) T.stream_inv += (size_t)c * (kIStageBytes / 2);
+    }
     // Tile costs in pipeline chunks, plus a fixed epilogue of about seven
     // chunks per tile.  Without the resident table, a chunk whose degrees
     // start below the order's largest first significant degree takes the
@@ -1389,6 +1394,13 @@ int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_gra
 int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes) {
     if (!plan || !bytes) return set_err(HPX_ERR_INVALID_ARG, "null argument");
     *bytes = plan->tc.table ? plan->tc.table_bytes : 0;
+    return HPX_OK;
+}
+
+int hpx_plan_table_stream_bytes(hpx_plan_t plan, size_t* fwd, size_t* inv) {
+    if (!plan || !fwd || !inv) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    *fwd = plan->tc.table ? plan->tc.stream_fwd : 0;
+    *inv = plan->tc.table ? plan->tc.stream_inv : 0;
     return HPX_OK;
 }
 

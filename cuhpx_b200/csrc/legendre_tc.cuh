@@ -153,6 +153,7 @@ struct TcPlan {
     int table = 0;            // 1: Pbar read from the resident table, 0: generated by producer warps
     int Lt = 0;               // table row length (halves)
     size_t table_bytes = 0;
+    size_t stream_fwd = 0, stream_inv = 0;  // table bytes one pass streams (TMA boxes of the tiles' chunks)
     uint16_t* d_table = nullptr;  // [m_tc_end][2 par][2 hl][2N][Lt]
     CUtensorMap tab_fwd{}, tab_inv{};
     int Lh = 0;               // rows per (m, parity) of the synthesis operand

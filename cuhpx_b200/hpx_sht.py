@@ -95,6 +95,14 @@ class Plan:
         _lib.check(self._lib.hpx_plan_table_bytes(self._h, ctypes.byref(n)), self._h)
         return n.value
 
+    @property
+    def table_stream_bytes(self):
+        """(analysis, synthesis): table bytes one pass over a chunk of maps streams
+        (all-zero table blocks are skipped); (0, 0) without a table."""
+        f, i = ctypes.c_size_t(), ctypes.c_size_t()
+        _lib.check(self._lib.hpx_plan_table_stream_bytes(self._h, ctypes.byref(f), ctypes.byref(i)), self._h)
+        return f.value, i.value
+
     # ------------------------------------------------------------------ stats
     def stats_enable(self, on=True):
         _lib.check(self._lib.hpx_stats_enable(self._h, 1 if on else 0), self._h)

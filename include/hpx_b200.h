@@ -200,6 +200,13 @@ HPX_API int hpx_plan_create_latlon(const hpx_latlon_desc_t* desc, hpx_plan_t* pl
 /* Bytes of the plan's resident Legendre table (0 when it has none). */
 HPX_API int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes);
 
+/* Table bytes one analysis (fwd) and one synthesis (inv) pass over a chunk of
+ * maps streams: the table's blocks that hold a nonzero entry for some tile
+ * (all-zero blocks, at polar rings below the turning point, are skipped).
+ * 0 and 0 when the plan has no table.  Introspection for roofline accounting;
+ * no counterpart in cuHPX. */
+HPX_API int hpx_plan_table_stream_bytes(hpx_plan_t plan, size_t* fwd, size_t* inv);
+
 /* Plan geometry queries. */
 HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);
 
