@@ -513,14 +513,14 @@ def algorithmic(nside, L, M):
 # table, from one single-pass ncu capture of this script's default workload:
 # stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
 MEASURED_TRAFFIC = {
-    "ring_fft_forward": (2152408576 + 2101460992) + (1231005440 + 1028252416),
-    "ring_fft_inverse": (2151525888 + 2112886016) + (1232021248 + 1027889920),
-    "fold": 3221534208 + 3172663296,
-    "legendre_forward": 19294675200 + 1070779392,
-    "columns_to_alm": 1088915456 + 2099540736,
-    "alm_to_columns": (1089042432 + 132096) + (1088926464 + 1077800960),
-    "legendre_inverse": 17085071360 + 3165193984,
-    "unfold": 3230080000 + 3172550656,
+    "ring_fft_forward": (2152460800 + 2101952512) + (1230765568 + 1027902976),
+    "ring_fft_inverse": (2151499776 + 2111714560) + (1232396288 + 1028977664),
+    "fold": 3221472256 + 3171683072,
+    "legendre_forward": 19662799104 + 1066859008,
+    "columns_to_alm": 1088933120 + 2099527680,
+    "alm_to_columns": (1088931840 + 1879296) + (1088917248 + 1078230016),
+    "legendre_inverse": 16853736448 + 3177124864,
+    "unfold": 3230082304 + 3175605760,
 }
 
 # kernels behind each stage's timer: the ring stages launch the power-of-two
