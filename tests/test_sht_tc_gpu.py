@@ -160,3 +160,22 @@ def test_table_matches_on_the_fly(hpx, cuda, prec):
     gt = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=True)(at)
     go = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec, legendre_table=False)(at)
     assert rel(gt, go.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
+def test_table_stream_bytes(hpx, cuda, prec):
+    """A table plan streams at most its box-granular table per pass and skips
+    all-zero blocks (more of them with fp16, whose smallest subnormal is far
+    above bf16's); an on-the-fly plan reports (0, 0)."""
+    nside, L = 256, 511
+    p = hpx.get_plan(nside, L, L, "ring", prec, cuda.index, legendre_table=True)
+    fwd, inv = p.table_stream_bytes
+    assert p.table_bytes > 0 and 0 < fwd and 0 < inv
+    # box-granular bound: every analysis tile's full ring range, every synthesis tile's full degree range
+    assert fwd <= 2 * p.table_bytes and inv <= 2 * p.table_bytes
+    q = hpx.get_plan(nside, L, L, "ring", prec, cuda.index, legendre_table=False)
+    assert q.table_stream_bytes == (0, 0)
+    if prec == "f16x3":
+        b = hpx.get_plan(nside, L, L, "ring", "bf16x3", cuda.index, legendre_table=True)
+        bf, bi = b.table_stream_bytes
+        assert fwd <= bf and inv <= bi
