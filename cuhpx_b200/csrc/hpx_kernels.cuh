@@ -348,21 +348,40 @@ __global__ void k_alm_to_cols(const T* __restrict__ alm, int nmaps, int L, int M
     }
 }
 
+// twiddles e^{-2 pi i q/P} read straight from the plan's FP64 table for Pmax
+struct StrideTw64 {
+    const cplx<double>* p;
+    int stride;
+    __device__ __forceinline__ cplx<double> operator()(int q) const { return p[q * stride]; }
+};
+
 // Bluestein tables per ring pair (FP64, rounded to T):
 //   chirp[j] = e^{-i pi j^2/h}, j < h  (phase from the integer j^2 mod 2h)
 //   G = FFT_P(g) / P in natural order, g_j = e^{+i pi j^2/h} for |j| < h (wrapped)
-template <typename T>
+// The FP64 FFT runs in shared memory, or (GLOBAL, when two FP64 buffers of
+// the largest P do not fit there: nside 2048) in a global scratch of
+// 2 padded_len(Pmax) elements per block.  Plan creation only.
+template <typename T, bool GLOBAL>
 __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restrict__ pairs,
                                                        const cplx<double>* __restrict__ tw64, int logPmax,
-                                                       cplx<T>* __restrict__ gtab, cplx<T>* __restrict__ chirp) {
+                                                       cplx<T>* __restrict__ gtab, cplx<T>* __restrict__ chirp,
+                                                       cplx<double>* __restrict__ scratch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const RingPair rp = pairs[blockIdx.x];
     if (rp.logh >= 0) return;
-    cplx<double>* buf = (cplx<double>*)smem_raw;
-    cplx<double>* buf2 = buf + padded_len(1 << rp.logP);
-    cplx<double>* twP = buf2 + padded_len(1 << rp.logP);
     const int P = 1 << rp.logP, h = rp.h;
-    load_twiddles(twP, rp.logP, tw64, logPmax);
+    cplx<double>* buf;
+    cplx<double>* buf2;
+    cplx<double>* twP = nullptr;
+    if constexpr (GLOBAL) {
+        buf = scratch + (size_t)blockIdx.x * 2 * padded_len(1 << logPmax);
+        buf2 = buf + padded_len(1 << logPmax);
+    } else {
+        buf = (cplx<double>*)smem_raw;
+        buf2 = buf + padded_len(P);
+        twP = buf2 + padded_len(P);
+        load_twiddles(twP, rp.logP, tw64, logPmax);
+    }
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         const int d = j < h ? j : (j > P - h ? P - j : -1);
         cplx<double> v = {0.0, 0.0};
@@ -376,8 +395,13 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
         if (j < h) chirp[rp.gtab_off + j] = {(T)v.re, (T)(-v.im)};
     }
     __syncthreads();
-    cplx<double>* r = fft_pow2<double, false>(buf, buf2, rp.logP, FullTw<double>{twP}, threadIdx.x, blockDim.x, 0,
-                                              IdentityMap{}, IdentityMap{});
+    cplx<double>* r;
+    if constexpr (GLOBAL)
+        r = fft_pow2<double, false>(buf, buf2, rp.logP, StrideTw64{tw64, 1 << (logPmax - rp.logP)}, threadIdx.x,
+                                    blockDim.x, 0, IdentityMap{}, IdentityMap{});
+    else
+        r = fft_pow2<double, false>(buf, buf2, rp.logP, FullTw<double>{twP}, threadIdx.x, blockDim.x, 0, IdentityMap{},
+                                    IdentityMap{});
     const double inv = 1.0 / (double)P;
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         gtab[rp.gtab_off + j] = {(T)(r[padi(j)].re * inv), (T)(r[padi(j)].im * inv)};

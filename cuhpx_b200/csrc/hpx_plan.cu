@@ -227,12 +227,24 @@ int create_typed(hpx_plan_s* P) {
         size_t sm = (size_t)(2 * padded_len(Pmax) + padded_len(Pmax / 2)) * sizeof(cplx<double>);
         int dmax = 0;
         HPX_CUDA_TRY(cudaDeviceGetAttribute(&dmax, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
-        if ((int)sm > dmax) return set_err(HPX_ERR_UNSUPPORTED, "nside too large for the chirp precompute");
-        HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmax));
-        k_chirp_spectra<T><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab, (C*)P->d_chirp);
+        cplx<double>* scratch = nullptr;
+        if ((int)sm <= dmax) {
+            HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmax));
+            k_chirp_spectra<T, false><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab, (C*)P->d_chirp,
+                                                          nullptr);
+        } else {
+            const size_t n = (size_t)P->NP * 2 * padded_len(Pmax);
+            if (cudaMalloc(&scratch, n * sizeof(cplx<double>)) != cudaSuccess) {
+                cudaFree(tw64);
+                return set_err(HPX_ERR_OOM, "chirp precompute scratch");
+            }
+            k_chirp_spectra<T, true><<<P->NP, 256>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab, (C*)P->d_chirp,
+                                                     scratch);
+        }
         cudaError_t e = cudaGetLastError();
         cudaError_t e2 = cudaDeviceSynchronize();
         cudaFree(tw64);
+        cudaFree(scratch);
         if (e != cudaSuccess || e2 != cudaSuccess)
             return set_err(HPX_ERR_CUDA, std::string("chirp spectra: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
     }

@@ -344,3 +344,20 @@ def test_conjugated_inputs_and_cotangents(cuda):
     g = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(a.detach().conj())
     g2 = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(a.detach().conj().resolve_conj())
     assert torch.equal(g, g2)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 5e-6), ("f16x3", 1e-5)])
+def test_nside_2048_band_limited_round_trip(hpx, cuda, prec, tol):
+    """nside 2048: Bluestein lengths up to 8192 (their FP64 chirp spectra are
+    precomputed in a global scratch) and shared-memory ring kernels near the
+    per-block limit; synthesis then analysis of band-limited coefficients
+    returns them."""
+    nside, L = 2048, 255
+    rng = np.random.default_rng(2048)
+    a = (rng.standard_normal((1, L, L)) + 1j * rng.standard_normal((1, L, L))) / np.sqrt(np.arange(1, L + 1))[None, :, None]
+    a = np.tril(a)
+    a[:, :, 0] = a[:, :, 0].real
+    at = torch.from_numpy(a).to(cuda, torch.complex64)
+    f = hpx.iSHTCUDA(nside, lmax=L, mmax=L, precision=prec)(at)
+    b = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, refine_iters=0)(f)
+    assert rel(b, a) < tol
