@@ -8,10 +8,11 @@ namespace hpx {
 
 // complex elements of dynamic shared memory the ring kernels need
 // (the phase and twiddle tables, and the padded work buffers of every FFT
-// group: groups x P <= 4096 whenever P <= 4096)
+// group: groups x P <= 4096 whenever P <= 4096, so the groups' 2 padded_len(P)
+// each take at most 2 padded_len(4096) + 32; 64 of slack)
 __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
     return (size_t)phase_tab_elems(nmax) + (size_t)phase_tab_elems(pfft_max / 2) +
-           2 * (size_t)padded_len(pfft_max > 4096 ? pfft_max : 4096) + 16;
+           2 * (size_t)padded_len(pfft_max > 4096 ? pfft_max : 4096) + 64;
 }
 
 // CTAs per SM the ring kernels are compiled for: 3 x 256 threads of float
@@ -48,7 +49,7 @@ __device__ __forceinline__ cplx<T>* ring_bluestein_tables(cplx<T>* smem, const R
     for (int i = threadIdx.x; i < rp.h; i += blockDim.x) csm[i] = chirp[rp.gtab_off + i];
     Gs = gsm;
     cs = csm;
-    return csm + rp.h;
+    return csm + rp.h + ((half + rp.h) & 1);  // the buffers start 16-byte aligned
 }
 
 // The ring kernels come in two instantiations launched over two ring lists:

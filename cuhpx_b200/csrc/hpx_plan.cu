@@ -251,7 +251,7 @@ int create_typed(hpx_plan_s* P) {
     // shared memory budgets
     P->ring_smem = ring_smem_elems(P->bufP, P->nmax) * sizeof(C);
     // Bluestein CTAs also hold the ring's chirp and half of its chirp spectrum
-    P->blue_smem = P->n_rings_blue ? (ring_smem_elems(P->bufP, P->nmax) + P->pblue / 2 + 1 + P->hblue) * sizeof(C) : 0;
+    P->blue_smem = P->n_rings_blue ? (ring_smem_elems(P->bufP, P->nmax) + P->pblue / 2 + 2 + P->hblue) * sizeof(C) : 0;
     P->fwd_smem = fwd_smem_bytes<T>();
     P->inv_smem = inv_smem_bytes<T>(P->L);
     int dev_max = 0;

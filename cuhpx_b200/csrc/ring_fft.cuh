@@ -53,9 +53,10 @@ struct RingPair {
 };
 
 // FFT work buffers are padded by one element every 16 so that the strided
-// Stockham stores of the first pass (stride 16 complex) spread over all banks.
+// Stockham stores of the first pass (stride 16 complex) spread over all banks;
+// their length is even, so that consecutive buffers stay 16-byte aligned.
 __device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int padded_len(int P) { return P + (P >> 4) + 1; }
+__host__ __device__ constexpr int padded_len(int P) { return (P + (P >> 4) + 2) & ~1; }
 
 // ----------------------------------------------------------------- sync helpers
 // Threads [g*tpf, (g+1)*tpf) of the CTA form FFT group g.
@@ -336,7 +337,10 @@ __device__ __forceinline__ int padi_step(int pi, int i, int r) {
 // ZIN: the input is zero from P/2 on (the first pass then loads and transforms
 // only R/2 of its R inputs); HOUT: only outputs below P/2 are wanted (the last
 // pass forms and stores only those).  Bluestein's convolution has both.
-template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT,
+// UNPAD: the last pass stores in natural, unpadded order (its stores are
+// consecutive across a warp, so the padding buys nothing there) -- the inverse
+// ring transform then copies its result out with 16-byte accesses.
+template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT, bool UNPAD,
           typename TW, typename Pre, typename Post>
 __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, Pre& pre,
                                             Post& post) {
@@ -374,37 +378,40 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
             if (LAST && HOUT && 2 * r >= R) continue;  // o + r NS >= P/2
             cplx<T> x = v[r];
             if constexpr (LAST) x = post(o + r * NS, x);
-            dst[padi_step<NS>(po, o, r)] = x;
+            if constexpr (LAST && UNPAD)
+                dst[o + r * NS] = x;
+            else
+                dst[padi_step<NS>(po, o, r)] = x;
         }
     }
 }
 
 // radix-16 passes NS, 16 NS, ... until the length is P
-template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, typename TW, typename Pre,
-          typename Post>
+template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, bool UNPAD, typename TW,
+          typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
                                                Post& post) {
     if constexpr (NS >= P) {
         return src;
     } else {
         constexpr bool LAST = NS * 16 == P;
-        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT>(src, dst, tw, lt, pre, post);
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT, UNPAD>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT>(dst, src, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT, UNPAD>(dst, src, tw, lt, g, pre, post);
     }
 }
 
-template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, typename TW, typename Pre, typename Post>
+template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, bool UNPAD, typename TW, typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
                                            Post& post) {
     constexpr int P = 1 << LOGP, TPF = fft_tpf(P), R0 = 1 << (LOGP & 3);
     if constexpr (R0 > 1) {
         constexpr bool LAST = R0 == P;
-        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT>(src, dst, tw, lt, pre, post);
+        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT, UNPAD>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT>(dst, src, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT, UNPAD>(dst, src, tw, lt, g, pre, post);
     } else {
-        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
     }
 }
 
@@ -415,26 +422,37 @@ __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW&
 // (tw, pre and post by value: this function may not be inlined, and a
 // reference would make every twiddle lookup reload the table's pointers from
 // the stack)
-template <typename T, bool INV, bool ZIN = false, bool HOUT = false, typename TW, typename Pre, typename Post>
+template <typename T, bool INV, bool ZIN = false, bool HOUT = false, bool UNPAD = false, typename TW, typename Pre,
+          typename Post>
 __device__ __forceinline__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const TW tw, int lt, int tpf, int g,
                                              Pre pre, Post post) {
-    if (tpf != fft_tpf(1 << logP)) return fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
-    switch (logP) {
-        case 1: return fft_ct<T, INV, 1, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 2: return fft_ct<T, INV, 2, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 3: return fft_ct<T, INV, 3, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 4: return fft_ct<T, INV, 4, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 5: return fft_ct<T, INV, 5, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 6: return fft_ct<T, INV, 6, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 7: return fft_ct<T, INV, 7, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 8: return fft_ct<T, INV, 8, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 9: return fft_ct<T, INV, 9, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 10: return fft_ct<T, INV, 10, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 11: return fft_ct<T, INV, 11, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 12: return fft_ct<T, INV, 12, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        case 13: return fft_ct<T, INV, 13, ZIN, HOUT>(src, dst, tw, lt, g, pre, post);
-        default: return fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
+    if (tpf == fft_tpf(1 << logP)) {
+        switch (logP) {
+            case 1: return fft_ct<T, INV, 1, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 2: return fft_ct<T, INV, 2, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 3: return fft_ct<T, INV, 3, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 4: return fft_ct<T, INV, 4, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 5: return fft_ct<T, INV, 5, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 6: return fft_ct<T, INV, 6, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 7: return fft_ct<T, INV, 7, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 8: return fft_ct<T, INV, 8, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 9: return fft_ct<T, INV, 9, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 10: return fft_ct<T, INV, 10, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 11: return fft_ct<T, INV, 11, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 12: return fft_ct<T, INV, 12, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 13: return fft_ct<T, INV, 13, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            default: break;
+        }
     }
+    // generic passes (padded output); UNPAD: copied into the other buffer unpadded
+    cplx<T>* r = fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
+    if constexpr (UNPAD) {
+        cplx<T>* o = (r == src) ? dst : src;
+        for (int j = lt; j < (1 << logP); j += tpf) o[j] = r[padi(j)];
+        group_sync(tpf, g);
+        return o;
+    }
+    return r;
 }
 
 // twP[padi(q)] = e^{-2 pi i q / P}, q < P/2, from the plan's table for Pmax
@@ -455,8 +473,9 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
     IdentityMap id;
     if constexpr (!BLUE) {
         // power-of-two ring
+        // (the inverse transform's result in natural unpadded order)
         if (rp.logh == 0) return buf;
-        return inv ? fft_ring<T, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
+        return inv ? fft_ring<T, true, false, false, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
                    : fft_ring<T, false>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id);
     } else {
         // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
@@ -483,7 +502,9 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
         cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
         cplx<T>* o = (r == buf) ? buf2 : buf;
-        return fft_ring<T, true, false, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
+        // (the inverse transform's result in natural unpadded order)
+        return inv ? fft_ring<T, true, false, true, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc)
+                   : fft_ring<T, true, false, true, false>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
     }
 }
 
@@ -597,13 +618,25 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
     cplx<T>* z = ring_dft<BLUE>(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
     load_next(freeb);
-    for (int j = lt; j < h; j += tpf) {
-        cplx<T> v = z[padi(j)];
-        if (ref) {
-            const cplx<T> rv = *(const cplx<T>*)(ref + 2 * j);
-            v = csub(rv, v);
+    // z holds the ring in natural unpadded order: two complex values per
+    // 16-byte access when both ends are aligned (HEALPix rings of an aligned map
+    // start at a multiple of 4 pixels)
+    bool vec = false;
+    if constexpr (sizeof(T) == 4)
+        vec = !ref && (h & 1) == 0 && ((((uintptr_t)x) | ((uintptr_t)z)) & 15) == 0;
+    if (vec) {
+        const float4* zs = (const float4*)z;
+        float4* xd = (float4*)x;
+        for (int j = lt; j < h / 2; j += tpf) xd[j] = zs[j];
+    } else {
+        for (int j = lt; j < h; j += tpf) {
+            cplx<T> v = z[j];
+            if (ref) {
+                const cplx<T> rv = *(const cplx<T>*)(ref + 2 * j);
+                v = csub(rv, v);
+            }
+            *(cplx<T>*)(x + 2 * j) = v;
         }
-        *(cplx<T>*)(x + 2 * j) = v;
     }
     group_sync(tpf, g);
     cur = freeb;
