@@ -20,16 +20,36 @@ __host__ __device__ constexpr size_t ring_smem_elems(int pfft_max, int nmax) {
 template <typename T>
 constexpr int ring_min_ctas() { return sizeof(T) == 4 ? 3 : 2; }
 
-// shared-memory layout of a ring CTA: phase table E (e^{-i pi q/nphi}), FFT
-// twiddles (e^{-2 pi i q/P}), then the work buffers
+// Per ring pair, the phase table E (e^{-i pi q/nphi}) and the FFT twiddles
+// (e^{-2 pi i q/P}) one after the other, built once per plan into a slot of
+// `slot` elements (k_ring_tables); each ring CTA copies its pair's slot.
 template <typename T>
-__device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingPair& rp, PhaseTab<T>& E,
-                                                PhaseTab<T>& tw) {
+__global__ void __launch_bounds__(256) k_ring_tables(const RingPair* __restrict__ pairs, int slot,
+                                                     cplx<T>* __restrict__ out) {
+    const RingPair rp = pairs[blockIdx.x];
+    cplx<T>* et = out + (size_t)blockIdx.x * slot;
+    build_phase_tab(et, rp.nphi);
+    if (rp.logP > 0) build_phase_tab(et + phase_tab_elems(rp.nphi), (1 << rp.logP) / 2);
+}
+
+// complex elements of a ring pair's table slot (nmax: the largest nphi)
+__host__ __device__ constexpr int ring_table_slot(int pfft_max, int nmax) {
+    return (phase_tab_elems(nmax) + phase_tab_elems(pfft_max / 2) + 1) & ~1;
+}
+
+// shared-memory layout of a ring CTA: phase table E, FFT twiddles (copied from
+// the pair's slot), then the work buffers
+template <typename T>
+__device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingPair& rp,
+                                                const cplx<T>* __restrict__ slot, PhaseTab<T>& E, PhaseTab<T>& tw) {
     cplx<T>* et = (cplx<T>*)smem;
-    cplx<T>* tt = et + phase_tab_elems(rp.nphi);
-    E = build_phase_tab(et, rp.nphi);
+    const int ne = phase_tab_elems(rp.nphi);
     const int half = (1 << rp.logP) / 2;
-    tw = rp.logP > 0 ? build_phase_tab(tt, half) : E;  // no FFT when h = 1
+    const int n = ne + (rp.logP > 0 ? phase_tab_elems(half) : 0);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) et[i] = slot[i];
+    E = PhaseTab<T>{et, et + 64, phase_tab_nhi(rp.nphi)};
+    cplx<T>* tt = et + ne;
+    tw = rp.logP > 0 ? PhaseTab<T>{tt, tt + 64, phase_tab_nhi(half)} : E;  // no FFT when h = 1
     return tt + phase_tab_elems(half);
 }
 
@@ -64,15 +84,17 @@ constexpr int ring_kernel_ctas() { return BLUE ? 2 : ring_min_ctas<T>(); }
 template <typename T, bool BLUE>
 __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta, T* __restrict__ F, int64_t Ftot, Geom geo,
-               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ gtab,
-               const cplx<T>* __restrict__ chirp, unsigned* __restrict__ fmax) {
+               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ rtab,
+               int rslot, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+               unsigned* __restrict__ fmax) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
     const int t = rings[blockIdx.x];
     const bool south = t >= NP;
-    const RingPair rp = pairs[south ? R - 1 - t : t];
+    const int pr = south ? R - 1 - t : t;
+    const RingPair rp = pairs[pr];
     PhaseTab<T> E, tw;
-    cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
+    cplx<T>* bufs = ring_tables(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
     const cplx<T>* Gs = nullptr;
     const cplx<T>* cs = nullptr;
     if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);
@@ -112,15 +134,17 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
 template <typename T, bool BLUE>
 __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map, int nmaps, int maps_per_cta, Geom geo,
-               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ gtab,
-               const cplx<T>* __restrict__ chirp, const T* __restrict__ ref) {
+               const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ rtab,
+               int rslot, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
+               const T* __restrict__ ref) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int NP = geo.NP, R = geo.R;
     const int t = rings[blockIdx.x];
     const bool south = t >= NP;
-    const RingPair rp = pairs[south ? R - 1 - t : t];
+    const int pr = south ? R - 1 - t : t;
+    const RingPair rp = pairs[pr];
     PhaseTab<T> E, tw;
-    cplx<T>* bufs = ring_tables(smem_raw, rp, E, tw);
+    cplx<T>* bufs = ring_tables(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
     const cplx<T>* Gs = nullptr;
     const cplx<T>* cs = nullptr;
     if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);

@@ -99,6 +99,8 @@ struct hpx_plan_s {
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     mutable std::mutex fork_mu;
+    void* d_rtab = nullptr; // cplx<T> per ring pair: phase table and FFT twiddles (ring_table_slot elements)
+    int rslot = 0;
     void* d_gtab = nullptr; // cplx<T> Bluestein chirp spectra (natural order)
     void* d_chirp = nullptr; // cplx<T> Bluestein chirps
     int64_t Ftot = 0;        // complex spectrum entries per map over all rings
@@ -152,6 +154,7 @@ struct hpx_plan_s {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         cudaFree(d_gtab);
+        cudaFree(d_rtab);
         cudaFree(d_chirp);
         cudaFree(d_lstart);
         cudaFree(d_pstart);
@@ -248,6 +251,11 @@ int create_typed(hpx_plan_s* P) {
         if (e != cudaSuccess || e2 != cudaSuccess)
             return set_err(HPX_ERR_CUDA, std::string("chirp spectra: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
+    // per ring pair: phase table and FFT twiddles, copied by each ring CTA
+    P->rslot = ring_table_slot(P->bufP, P->nmax);
+    HPX_CUDA_TRY(cudaMalloc(&P->d_rtab, (size_t)P->NP * P->rslot * sizeof(C)));
+    k_ring_tables<T><<<P->NP, 256>>>(P->d_pairs, P->rslot, (C*)P->d_rtab);
+    HPX_CUDA_TRY(cudaGetLastError());
     // shared memory budgets
     P->ring_smem = ring_smem_elems(P->bufP, P->nmax) * sizeof(C);
     // Bluestein CTAs also hold the ring's chirp and half of its chirp spectrum
@@ -956,14 +964,15 @@ struct Pipeline {
             const unsigned nbk = (nb + g - 1) / g;
             const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
             const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
+            const cplx<T>* rt = (const cplx<T>*)P->d_rtab;
             ring_launches(
                 [&](cudaStream_t s) {
                     k_ring_fwd<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
-                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, gt, ch, fmax);
+                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, rt, P->rslot, gt, ch, fmax);
                 },
                 [&](cudaStream_t s) {
                     k_ring_fwd<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
-                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, fmax);
+                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot, gt, ch, fmax);
                 });
         }
         Timer tm(P, st, kStFold);
@@ -985,14 +994,15 @@ struct Pipeline {
         const unsigned nbk = (nb + g - 1) / g;
         const cplx<T>* gt = (const cplx<T>*)P->d_gtab;
         const cplx<T>* ch = (const cplx<T>*)P->d_chirp;
+        const cplx<T>* rt = (const cplx<T>*)P->d_rtab;
         ring_launches(
             [&](cudaStream_t s) {
                 k_ring_inv<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
-                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, gt, ch, ref);
+                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, rt, P->rslot, gt, ch, ref);
             },
             [&](cudaStream_t s) {
                 k_ring_inv<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
-                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, gt, ch, ref);
+                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot, gt, ch, ref);
             });
     }
     void leg_fwd(T* alm, int nb, int accumulate) {
