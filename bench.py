@@ -513,14 +513,14 @@ def algorithmic(nside, L, M):
 # table, from one single-pass ncu capture of this script's default workload:
 # stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
 MEASURED_TRAFFIC = {
-    "ring_fft_forward": (2152460800 + 2101952512) + (1230765568 + 1027902976),
-    "ring_fft_inverse": (2151499776 + 2111714560) + (1232396288 + 1028977664),
-    "fold": 3221472256 + 3171683072,
-    "legendre_forward": 19662799104 + 1066859008,
-    "columns_to_alm": 1088933120 + 2099527680,
-    "alm_to_columns": (1088931840 + 1879296) + (1088917248 + 1078230016),
-    "legendre_inverse": 16853736448 + 3177124864,
-    "unfold": 3230082304 + 3175605760,
+    "ring_fft_forward": (2179299584 + 2098085120) + (1163196928 + 1027983616),
+    "ring_fft_inverse": (2178460672 + 2146554880) + (1164303616 + 1026849280),
+    "fold": 3221681408 + 3172218880,
+    "legendre_forward": 19416636160 + 1066140160,
+    "columns_to_alm": 1088008192 + 2099074560,
+    "alm_to_columns": (1088958720 + 59904) + (1088963072 + 1077838592),
+    "legendre_inverse": 17068165632 + 3178639360,
+    "unfold": 3230574080 + 3173698048,
 }
 
 # kernels behind each stage's timer: the ring stages launch the power-of-two
