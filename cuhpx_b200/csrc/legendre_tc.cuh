@@ -4,18 +4,20 @@
 // north/south folding, per-m contraction), mapped onto the 5th-generation
 // tensor cores:
 //
-//  * the Pbar operand is generated on the fly by producer warps running the
-//    FP64 three-term recurrence from the plan's 64-degree block seeds, rounded
-//    to FP32 and split into bf16 hi + lo, and stored straight into shared
-//    memory in the UMMA SWIZZLE_128B (analysis) / SWIZZLE_64B (synthesis)
-//    canonical layout;
+//  * the Pbar operand comes from the plan's resident table (fp16 or bf16 hi
+//    and lo halves) by TMA, or, without the table, is generated on the fly by
+//    producer warps running the FP64 three-term recurrence from the plan's
+//    64-degree block seeds, rounded to FP32, split into hi + lo and stored
+//    straight into shared memory; either way in the UMMA SWIZZLE_128B
+//    (analysis) / SWIZZLE_64B (synthesis) canonical layout;
 //  * the data operand (folded spectra for analysis, coefficients for
-//    synthesis) is pre-split into bf16 hi/lo in global memory and brought in by
-//    TMA (cp.async.bulk.tensor, 128B swizzle, no multicast);
+//    synthesis) is pre-split into hi/lo halves in global memory and brought in
+//    by TMA (cp.async.bulk.tensor, 128B swizzle, no multicast);
 //  * one thread issues tcgen05.mma (M=128, N=128, K=16) for the three products
 //    into FP32 accumulators in TMEM; tcgen05.commit frees a pipeline stage
 //    when its MMAs retire;
-//  * four epilogue warps drain TMEM (tcgen05.ld) and add the accumulators.
+//  * epilogue warps (four, or eight with the table) drain TMEM (tcgen05.ld)
+//    and add the accumulators.
 //
 // TMEM (512 columns) holds, per parity, a main accumulator (hi*hi) and a cross
 // accumulator (hi*lo + lo*hi), at column (2 par + part) * 128.  The tensor
@@ -28,7 +30,7 @@
 // round-to-nearest FP32.
 //
 // Analysis tile  = (m, 256 consecutive degrees): D_par[128 l][128 cols] +=
-//                   Pbar_par[128 l][32 rings] * X_par[32 rings][128 cols]
+//                   Pbar_par[128 l][16 or 32 rings] * X_par[rings][128 cols]
 // Synthesis tile = (m, 128 rings):   D_par[128 rings][128 cols] +=
 //                   Pbar^T[128 rings][32 l] * A_par[32 l][128 cols]
 // where par is the parity of l-m and cols = 2*map + {re, im}.

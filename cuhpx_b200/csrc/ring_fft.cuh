@@ -10,16 +10,18 @@
 //
 // Design (not the reference's): a real ring of length n = nphi is packed into
 // a complex sequence of length h = n/2.  If h is a power of two it goes
-// through a Stockham radix-4/2 FFT in shared memory, otherwise through
-// Bluestein's chirp-z convolution with a per-ring power-of-two size
-// P >= 2h-1 (the reference pads every ring to 8*nside).  Small rings are
-// transformed by sub-groups of a CTA (one warp, two, four or all eight) so
-// that every thread handles ~16 points whatever the ring length.
+// through a Stockham FFT in shared memory (one radix-2/4/8 pass, then radix-16
+// passes, specialised per length), otherwise through Bluestein's chirp-z
+// convolution with a per-ring power-of-two size P >= 2h-1 (the reference pads
+// every ring to 8*nside).  Small rings are transformed by sub-groups of a CTA
+// (one warp, two, four or all eight) so that every thread handles ~16 points
+// whatever the ring length.
 //
 // Phases are exact: the chirp e^{-i pi j^2/h} is tabulated per ring in the plan
 // from the integer j^2 mod 2h in FP64, and the real-FFT split and phase-shift
-// factors e^{-i pi q/n} (q <= 2n) come from a per-CTA FP64-built table --
-// never from a float "pi*j*j/n" as in hpx_fft_cuda.cu:1090.
+// factors e^{-i pi q/n} (q <= 2n) and the FFT twiddles come from two-level
+// tables built in FP64 once per plan and ring pair -- never from a float
+// "pi*j*j/n" as in hpx_fft_cuda.cu:1090.
 //
 // Spectra are stored ring-major, F[map][foff_t + m] (m < mt_t), so every ring
 // reads and writes contiguous memory; separate fold/unfold kernels (in
