@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison run")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error check against the FP64 path")
+    ap.add_argument("--no-refined", action="store_true",
+                    help="skip the refined variants (1 and 3 Jacobi iterations) of the mixed-precision analysis")
     ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged"],
                     help="sht_isht: the headline step; ragged: 96 maps of mixed nside (analysis only)")
     ap.add_argument("--accuracy-maps", type=int, default=2)
@@ -328,6 +330,30 @@ def run_gpu(args):
     if not args.no_accuracy:
         acc = accuracy_vs_fp64(torch, hpx, sht, isht, f[: args.accuracy_maps], nside, L, refine)
 
+    # the workload's refined variants: k Jacobi iterations in the analysis (each
+    # one more synthesis and analysis of the residual), the same maps, and their
+    # round-trip error against the FP64 path with the same k
+    refined = None
+    if not args.no_refined and prec in ("f16x3", "bf16x3") and world == 1:
+        refined = {}
+        for k in (1, 3):
+            sht_k = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec, refine_iters=k)
+
+            def step_k():
+                with torch.no_grad():
+                    out["fk"] = isht(sht_k(f))
+
+            ms_k = time_steps(torch, step_k, max(2, args.steps // 2), args.warmup, dist, stream)
+            e = {"maps_per_s": B * max(2, args.steps // 2) / (ms_k / 1000.0)}
+            if not args.no_accuracy:
+                a_k = accuracy_vs_fp64(torch, hpx, sht_k, isht, f[: args.accuracy_maps], nside, L, k)
+                e["roundtrip_rel_l2"] = a_k["roundtrip_rel_l2"]
+                e["alm_rel_l2"] = a_k["alm_rel_l2"]
+            refined[str(k)] = e
+            del sht_k
+        out.pop("fk", None)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(nside, L, args.cpu_sample_m)
@@ -367,6 +393,7 @@ def run_gpu(args):
             "plain_fp32_maps_per_s": plain,
             "check_rel_l2_vs_fp32": check_rel,
             "err_vs_fp64": acc,
+            "refined": refined,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
