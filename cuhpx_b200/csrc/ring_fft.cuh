@@ -341,9 +341,11 @@ __device__ __forceinline__ int padi_step(int pi, int i, int r) {
 // pass forms and stores only those).  Bluestein's convolution has both.
 // UNPAD: the last pass stores in natural, unpadded order (its stores are
 // consecutive across a warp, so the padding buys nothing there) -- the inverse
-// ring transform then copies its result out with 16-byte accesses.
+// ring transform then copies its result out with 16-byte accesses.  UNPIN:
+// likewise the first pass reads an unpadded input (the ring loads then move 16
+// bytes per copy).
 template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT, bool UNPAD,
-          typename TW, typename Pre, typename Post>
+          bool UNPIN, typename TW, typename Pre, typename Post>
 __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, Pre& pre,
                                             Post& post) {
     constexpr int Q = P / R;
@@ -361,7 +363,10 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
                 v[r] = {(T)0, (T)0};  // j + r Q >= P/2
                 continue;
             }
-            v[r] = src[padi_step<Q>(pj, j, r)];
+            if constexpr (FIRST && UNPIN)
+                v[r] = src[j + r * Q];
+            else
+                v[r] = src[padi_step<Q>(pj, j, r)];
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
         if constexpr (NS > 1) {
@@ -389,31 +394,32 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
 }
 
 // radix-16 passes NS, 16 NS, ... until the length is P
-template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, bool UNPAD, typename TW,
-          typename Pre, typename Post>
+template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, bool UNPAD, bool UNPIN,
+          typename TW, typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
                                                Post& post) {
     if constexpr (NS >= P) {
         return src;
     } else {
         constexpr bool LAST = NS * 16 == P;
-        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT, UNPAD>(src, dst, tw, lt, pre, post);
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT, UNPAD>(dst, src, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT, UNPAD, UNPIN>(dst, src, tw, lt, g, pre, post);
     }
 }
 
-template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, bool UNPAD, typename TW, typename Pre, typename Post>
+template <typename T, bool INV, int LOGP, bool ZIN, bool HOUT, bool UNPAD, bool UNPIN, typename TW, typename Pre,
+          typename Post>
 __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
                                            Post& post) {
     constexpr int P = 1 << LOGP, TPF = fft_tpf(P), R0 = 1 << (LOGP & 3);
     if constexpr (R0 > 1) {
         constexpr bool LAST = R0 == P;
-        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT, UNPAD>(src, dst, tw, lt, pre, post);
+        fft_pass_ct<T, INV, R0, 1, P, TPF, true, LAST, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
-        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT, UNPAD>(dst, src, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, R0, false, ZIN, HOUT, UNPAD, UNPIN>(dst, src, tw, lt, g, pre, post);
     } else {
-        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+        return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
     }
 }
 
@@ -424,29 +430,38 @@ __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW&
 // (tw, pre and post by value: this function may not be inlined, and a
 // reference would make every twiddle lookup reload the table's pointers from
 // the stack)
-template <typename T, bool INV, bool ZIN = false, bool HOUT = false, bool UNPAD = false, typename TW, typename Pre,
-          typename Post>
+template <typename T, bool INV, bool ZIN = false, bool HOUT = false, bool UNPAD = false, bool UNPIN = false, typename TW,
+          typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int logP, const TW tw, int lt, int tpf, int g,
                                              Pre pre, Post post) {
     if (tpf == fft_tpf(1 << logP)) {
         switch (logP) {
-            case 1: return fft_ct<T, INV, 1, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 2: return fft_ct<T, INV, 2, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 3: return fft_ct<T, INV, 3, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 4: return fft_ct<T, INV, 4, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 5: return fft_ct<T, INV, 5, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 6: return fft_ct<T, INV, 6, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 7: return fft_ct<T, INV, 7, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 8: return fft_ct<T, INV, 8, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 9: return fft_ct<T, INV, 9, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 10: return fft_ct<T, INV, 10, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 11: return fft_ct<T, INV, 11, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 12: return fft_ct<T, INV, 12, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
-            case 13: return fft_ct<T, INV, 13, ZIN, HOUT, UNPAD>(src, dst, tw, lt, g, pre, post);
+            case 1: return fft_ct<T, INV, 1, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 2: return fft_ct<T, INV, 2, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 3: return fft_ct<T, INV, 3, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 4: return fft_ct<T, INV, 4, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 5: return fft_ct<T, INV, 5, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 6: return fft_ct<T, INV, 6, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 7: return fft_ct<T, INV, 7, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 8: return fft_ct<T, INV, 8, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 9: return fft_ct<T, INV, 9, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 10: return fft_ct<T, INV, 10, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 11: return fft_ct<T, INV, 11, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 12: return fft_ct<T, INV, 12, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+            case 13: return fft_ct<T, INV, 13, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
             default: break;
         }
     }
-    // generic passes (padded output); UNPAD: copied into the other buffer unpadded
+    // generic passes (padded input and output); UNPIN: the input is first
+    // copied into the other buffer padded; UNPAD: the result is copied into the
+    // other buffer unpadded
+    if constexpr (UNPIN) {
+        for (int j = lt; j < (1 << logP); j += tpf) dst[padi(j)] = src[j];
+        group_sync(tpf, g);
+        cplx<T>* t = src;
+        src = dst;
+        dst = t;
+    }
     cplx<T>* r = fft_pow2<T, INV>(src, dst, logP, tw, lt, tpf, g, pre, post);
     if constexpr (UNPAD) {
         cplx<T>* o = (r == src) ? dst : src;
@@ -477,8 +492,8 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         // power-of-two ring
         // (the inverse transform's result in natural unpadded order)
         if (rp.logh == 0) return buf;
-        return inv ? fft_ring<T, true, false, false, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
-                   : fft_ring<T, false>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id);
+        return inv ? fft_ring<T, true, false, false, true, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id)
+                   : fft_ring<T, false, false, false, false, true>(buf, buf2, rp.logh, tw, lt, tpf, g, id, id);
     } else {
         // Bluestein, c_j = e^{-i pi j^2/h}: Z_k = c_k sum_j (z_j c_j) conj(c_{k-j}), the
         // convolution done as IFFT(FFT(z c) G) with G the plan's FFT of conj(c)
@@ -502,7 +517,7 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
             return v;
         };
         // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
-        cplx<T>* r = fft_ring<T, false, true, false>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
+        cplx<T>* r = fft_ring<T, false, true, false, false, true>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
         cplx<T>* o = (r == buf) ? buf2 : buf;
         // (the inverse transform's result in natural unpadded order)
         return inv ? fft_ring<T, true, false, true, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc)
@@ -517,11 +532,19 @@ __device__ __forceinline__ void cp_async_cplx(cplx<T>* dst, const cplx<T>* src) 
     else cp_async16(dst, src);
 }
 
-// The group starts copying ring x[0..n) (h complex) into dst[padi(j)]; the copy
-// is one cp.async commit group of the calling threads.
+// The group starts copying ring x[0..n) (h complex) into dst[0..h) (unpadded:
+// the first FFT pass reads it with consecutive addresses), two complex values
+// per 16-byte copy when both ends allow; the copy is one cp.async commit group
+// of the calling threads.
 template <typename T>
 __device__ __forceinline__ void ring_load_async(cplx<T>* dst, const T* x, int h, int lt, int tpf) {
-    for (int j = lt; j < h; j += tpf) cp_async_cplx(dst + padi(j), (const cplx<T>*)x + j);
+    bool vec = false;
+    if constexpr (sizeof(T) == 4) vec = (h & 1) == 0 && ((((uintptr_t)x) | ((uintptr_t)dst)) & 15) == 0;
+    if (vec) {
+        for (int j = lt; 2 * j < h; j += tpf) cp_async16(dst + 2 * j, x + 4 * j);
+    } else {
+        for (int j = lt; j < h; j += tpf) cp_async_cplx(dst + j, (const cplx<T>*)x + j);
+    }
     cp_async_commit();
 }
 
@@ -533,7 +556,7 @@ __device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg,
 }
 
 // Forward transform of one real ring into F[0..mt) (global, contiguous).  The
-// ring was loaded into cur[padi(j)] by ring_load_async; the two FFT buffers
+// ring was loaded into cur[j] by ring_load_async; the two FFT buffers
 // alternate roles from map to map: once the DFT is done, the buffer it left
 // free receives the next map's ring (load_next, asynchronous) while this map's
 // spectrum is formed and stored.  On return cur holds the next input.
@@ -614,8 +637,8 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
         }
         const cplx<T> sum = cadd(Xa, Xb), dif = csub(Xa, Xb);
         const cplx<T> r = cmul(cconj(E(2 * k)), dif);  // e^{+2 pi i k/n} (Xa - Xb)
-        buf[padi(k)] = {sum.re - r.im, sum.im + r.re};  // sum + i r
-        if (k != 0 && kb != k) buf[padi(kb)] = {sum.re + r.im, r.re - sum.im};
+        buf[k] = {sum.re - r.im, sum.im + r.re};  // sum + i r (unpadded: the FFT's first pass reads it)
+        if (k != 0 && kb != k) buf[kb] = {sum.re + r.im, r.re - sum.im};
     }
     cplx<T>* z = ring_dft<BLUE>(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
