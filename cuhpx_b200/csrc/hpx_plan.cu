@@ -715,7 +715,7 @@ int plan_build(hpx_plan_s* P) {
         const bool south = t >= P->NP;
         RingPair& rp = P->h_pairs[south ? P->R - 1 - t : t];
         if (south) rp.foff_s = foff; else rp.foff_n = foff;
-        foff += rp.mt;
+        foff += (rp.mt + 1) & ~1;  // even offsets: every ring's spectrum starts 16-byte aligned
     }
     P->Ftot = foff;
     P->logPmax = logPmax;

@@ -551,7 +551,15 @@ __device__ __forceinline__ void ring_load_async(cplx<T>* dst, const T* x, int h,
 // ... and the spectrum Fg[0..mt) into dst[0..mt) (contiguous).
 template <typename T>
 __device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg, int mt, int lt, int tpf) {
-    for (int k = lt; k < mt; k += tpf) cp_async_cplx(dst + k, Fg + k);
+    bool vec = false;
+    if constexpr (sizeof(T) == 4) vec = ((((uintptr_t)Fg) | ((uintptr_t)dst)) & 15) == 0;
+    if (vec) {
+        // two complex values per 16-byte copy (spectra start at even offsets)
+        for (int k = lt; 2 * k + 1 < mt; k += tpf) cp_async16(dst + 2 * k, Fg + 2 * k);
+        if ((mt & 1) && lt == 0) cp_async_cplx(dst + mt - 1, Fg + mt - 1);
+    } else {
+        for (int k = lt; k < mt; k += tpf) cp_async_cplx(dst + k, Fg + k);
+    }
     cp_async_commit();
 }
 
