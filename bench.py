@@ -540,14 +540,14 @@ def algorithmic(nside, L, M):
 # table, from one single-pass ncu capture of this script's default workload:
 # stage -> bytes.  Used for (nside, lmax, precision, batch) = (1024, 2047, f16x3, 64) only.
 MEASURED_TRAFFIC = {
-    "ring_fft_forward": (2179299584 + 2098085120) + (1163196928 + 1027983616),
-    "ring_fft_inverse": (2178460672 + 2146554880) + (1164303616 + 1026849280),
-    "fold": 3221681408 + 3172218880,
-    "legendre_forward": 19416636160 + 1066140160,
-    "columns_to_alm": 1088008192 + 2099074560,
-    "alm_to_columns": (1088958720 + 59904) + (1088963072 + 1077838592),
-    "legendre_inverse": 17068165632 + 3178639360,
-    "unfold": 3230574080 + 3173698048,
+    "ring_fft_forward": (2183413760 + 2138995712) + (1166255872 + 1030015488),
+    "ring_fft_inverse": (2179128064 + 2158633472) + (1164670208 + 1028427776),
+    "fold": 3223599360 + 3172154880,
+    "legendre_forward": 19562228480 + 1066144256,
+    "columns_to_alm": 1088439040 + 2098970624,
+    "alm_to_columns": (1088928768 + 386304) + (1088931584 + 1077855744),
+    "legendre_inverse": 17077325824 + 3179270656,
+    "unfold": 3252765440 + 3185650688,
 }
 
 # kernels behind each stage's timer: the ring stages launch the power-of-two
