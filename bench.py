@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error check against the FP64 path")
     ap.add_argument("--no-refined", action="store_true",
                     help="skip the refined variants (1 and 3 Jacobi iterations) of the mixed-precision analysis")
-    ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged"],
-                    help="sht_isht: the headline step; ragged: 96 maps of mixed nside (analysis only)")
+    ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged", "remap"],
+                    help="sht_isht: the headline step; ragged: 96 maps of mixed nside; remap: NEST -> RING "
+                         "reordering of a batch of maps (with the other layout pairs beside it)")
     ap.add_argument("--accuracy-maps", type=int, default=2)
     ap.add_argument("--cpu-sample-m", type=int, default=12)
     return ap.parse_args()
@@ -690,6 +691,100 @@ def run_ragged(args):
     return 0
 
 
+def run_remap(args):
+    """nest2ring of a batch of float32 maps (default 64 maps at nside 1024,
+    3.2 GB each way, larger than L2) per step, the operation the reference's
+    tests/reproduce_data_reorder_timing.py times (ms per map of a batched
+    call).  The roofline is HBM: every pixel is read once and written once.
+    Beside it: the other layout pairs, an end-to-end step through the public
+    API from and to pinned host memory, and the CPU restatement of the
+    reference's index formulas on one map."""
+    import torch
+
+    import cuhpx_b200 as hpx
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nside, B = args.nside, args.batch
+    npix = 12 * nside * nside
+    g = torch.Generator(device=dev)
+    g.manual_seed(6)
+    x = torch.randn((B, npix), generator=g, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def bench(fn):
+        return time_steps(torch, fn, args.steps, args.warmup, None, stream)
+
+    pairs = {
+        "nest2ring": lambda: hpx.nest2ring(x, nside),
+        "ring2nest": lambda: hpx.ring2nest(x, nside),
+        "nest2flat": lambda: hpx.nest2flat(x, "S", False, nside),
+        "ring2flat": lambda: hpx.ring2flat(x, "N", True, nside),
+        "flat2flat": lambda: hpx.flat2flat(x, "S", False, "E", True, nside),
+    }
+    sampler = ClockSampler(0)
+    sampler.start()
+    ms = bench(pairs["nest2ring"])
+    clocks = sampler.stop()
+    out = {name: (ms if name == "nest2ring" else bench(fn)) for name, fn in pairs.items()}
+    byts = 2.0 * npix * x.element_size() * B
+    hbm, _, source = load_peaks()
+    per_step = ms / args.steps
+    ach = byts / (per_step * 1e-3) / 1e9
+
+    # end to end: pinned host maps -> device -> nest2ring -> pinned host
+    host_in = torch.empty((B, npix), dtype=torch.float32, pin_memory=True)
+    host_in.copy_(x)
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    e2e_steps = max(3, min(args.steps, 10))
+
+    def e2e():
+        d = host_in.to(dev, non_blocking=True)
+        host_out.copy_(hpx.nest2ring(d, nside), non_blocking=True)
+
+    e2e_ms = time_steps(torch, e2e, e2e_steps, args.warmup, None, stream)
+    cpu = None
+    if not args.no_cpu:
+        from oracle import remap_oracle as R
+
+        one = x[0].cpu().numpy()
+        reps, t0 = 0, time.perf_counter()
+        while reps < 3 or time.perf_counter() - t0 < 10.0:
+            R.nest2ring(one, nside)
+            reps += 1
+        cpu_ms = (time.perf_counter() - t0) / reps * 1e3
+        cpu = {"value": 1e3 / cpu_ms, "unit": "maps/s", "cores": 1, "kind": "port",
+               "sample": f"oracle nest2ring (numpy, the reference's index formulas) of one nside-{nside} map, "
+                         f"{reps} repetitions"}
+    line = {
+        "metric": f"nest2ring maps/s nside{nside} B{B} float32",
+        "value": B / (per_step * 1e-3),
+        "unit": "maps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per_step,
+        "ms_per_map": per_step / B,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (bytes moved)",
+        "data": "synthetic",
+        "config": {"workload": f"nest2ring, {B} maps of nside {nside}", "nside": nside, "batch": B,
+                   "l2": f"inputs larger than L2 ({byts / 2e9:.2f} GB each way per step)"},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": None, "kernel": "k_remap_async", "peak_source": source, "algorithmic_bytes": byts},
+        "other_pairs_gbs": {k: byts / (v / args.steps * 1e-3) / 1e9 for k, v in out.items()},
+        "e2e": {"value": B * e2e_steps / (e2e_ms * 1e-3), "unit": "maps/s", "h2d_bytes_per_step": npix * 4 * B,
+                "d2h_bytes_per_step": npix * 4 * B, "steps": e2e_steps},
+        "gpu_launches": args.steps,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -698,6 +793,8 @@ def main():
         return run_reference(args)
     if args.workload == "ragged":
         return run_ragged(args)
+    if args.workload == "remap":
+        return run_remap(args)
     return run_gpu(args)
 
 

@@ -1,7 +1,9 @@
 """hpx_b200: HEALPix spherical-harmonic transforms for NVIDIA B200 (sm_100a).
 
 Drop-in for the SHT path of cuHPX: ``SHTCUDA``, ``iSHTCUDA``, ``Grid`` and
-``Regridding``.  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
+``Regridding``, and for its pixel-order remapping (``ring2nest``,
+``nest2ring``, ``nest2flat``, ``flat2nest``, ``ring2flat``, ``flat2ring``,
+``flat2flat``).  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
 C ABI in ``include/hpx_b200.h``); there is no CPU fallback.
 """
 
@@ -11,6 +13,7 @@ from .hpx_sht import (LatLonPlan, Plan, SHTCUDA, SHTFunction, clear_plan_cache, 
 from .latlon import InverseRealSHT, RealSHT
 from .ragged import RaggedISHT, RaggedSHT, split_by_offsets
 from .regrid import Grid, Regridding
+from .remap import flat2flat, flat2nest, flat2ring, nest2flat, nest2ring, ring2flat, ring2nest
 
 __all__ = [
     "SHTCUDA",
@@ -30,4 +33,11 @@ __all__ = [
     "get_plan",
     "clear_plan_cache",
     "sht_tools",
+    "ring2nest",
+    "nest2ring",
+    "nest2flat",
+    "flat2nest",
+    "ring2flat",
+    "flat2ring",
+    "flat2flat",
 ]

@@ -90,6 +90,8 @@ SIGNATURES = {
                             ctypes.POINTER(_i64), _vp, _sz, _vp], ctypes.c_int),
     "hpx_ragged_inverse": ([ctypes.POINTER(_vp), ctypes.c_int32, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                             ctypes.POINTER(_i64), _vp, _sz, _vp], ctypes.c_int),
+    "hpx_remap": ([_vp, _vp, _i64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                   ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp], ctypes.c_int),
     "hpx_plan_info": (
         [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
         ctypes.c_int,

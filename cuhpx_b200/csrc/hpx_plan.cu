@@ -35,6 +35,7 @@
 #include "../../include/hpx_b200.h"
 #include "hpx_kernels.cuh"
 #include "legendre_tc.cuh"
+#include "hpx_remap.cuh"
 
 using namespace hpx;
 
@@ -1214,9 +1215,126 @@ int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch,
     return HPX_OK;
 }
 
+// Opt a remap kernel into more than 48 KB of dynamic shared memory, once per
+// device.
+template <typename K>
+int remap_smem_optin(K kernel, size_t smem) {
+    if (smem <= 48 * 1024) return HPX_OK;
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    HPX_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && done[dev]) return HPX_OK;
+    HPX_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (dev < 64) done[dev] = true;
+    return HPX_OK;
+}
+
+// Remap launcher: squares of 64 x 64 pixels for elements of up to 4 bytes and
+// 32 x 32 above, fewer for nside < 64.  Map groups of up to 16 maps a CTA
+// amortise the offsets' arithmetic, while leaving at least 16 CTAs a
+// multiprocessor.  Elements of 4, 8 and 16 bytes take the cp.async pipeline;
+// 1- and 2-byte elements stage through registers.
+template <typename E>
+int launch_remap(const void* in, void* out, int64_t batch, int nside, RemapSide src, RemapSide dst,
+                 cudaStream_t st) {
+    const int logn = ilog2_exact(nside);
+    const int s = std::min(nside, sizeof(E) <= 4 ? 64 : 32);
+    const int logs = ilog2_exact(s);
+    const int log_tiles = logn - logs;
+    const int64_t tiles = 12ll << (2 * log_tiles);
+    int mpc = 16;
+    while (mpc > 1 && tiles * ((batch + mpc - 1) / mpc) < 148ll * 16) mpc >>= 1;
+    const bool ring = src.order == kOrderRing || dst.order == kOrderRing;
+    constexpr bool kAsync = sizeof(E) >= 4;
+    const size_t smem = kAsync ? remap_async_smem_bytes(s, (int)sizeof(E), ring)
+                               : remap_smem_bytes(s, (int)sizeof(E), ring);
+    if constexpr (kAsync) {
+        const int rc = remap_smem_optin(k_remap_async<E>, smem);
+        if (rc != HPX_OK) return rc;
+    }
+    const int64_t np = 12ll * nside * nside;
+    const int64_t chunk = 65535ll * mpc;
+    for (int64_t b = 0; b < batch; b += chunk) {
+        const int nb = (int)std::min(chunk, batch - b);
+        const dim3 grid((unsigned)tiles, (unsigned)((nb + mpc - 1) / mpc));
+        const E* pin = (const E*)in + b * np;
+        E* pout = (E*)out + b * np;
+        if constexpr (kAsync) {
+            k_remap_async<E><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
+                                                                dst);
+        } else {
+            if (s == 64)
+                k_remap<E, 16><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
+                                                                  dst);
+            else if (s == 32)
+                k_remap<E, 4><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
+                                                                 dst);
+            else
+                k_remap<E, 1><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
+                                                                 dst);
+        }
+        HPX_CUDA_TRY(cudaGetLastError());
+    }
+    return HPX_OK;
+}
+
+// (order, origin, clockwise) of one side -> its transform; XY faces rotate by
+// the origin counter-clockwise, or by minus the origin after the flip of a
+// clockwise face (src/data_remapping/hpx_remapping_cuda.cu:413-417)
+int remap_side(int32_t order, int32_t origin, int32_t clockwise, RemapSide* sd, const char* which) {
+    if (order < HPX_ORDER_RING || order > HPX_ORDER_XY)
+        return set_err(HPX_ERR_INVALID_ARG, std::string(which) + " order must be RING, NEST or XY");
+    sd->order = order;
+    sd->flip = 0;
+    sd->rot = 0;
+    if (order == HPX_ORDER_XY) {
+        if (origin < HPX_ORIGIN_S || origin > HPX_ORIGIN_W)
+            return set_err(HPX_ERR_INVALID_ARG, std::string("The ") + which + " origin must be one from S, E, N, W");
+        sd->flip = clockwise ? 1 : 0;
+        sd->rot = (clockwise ? -origin : origin) & 3;
+    }
+    return HPX_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, int32_t elem_bytes, int32_t src_order,
+              int32_t src_origin, int32_t src_clockwise, int32_t dst_order, int32_t dst_origin,
+              int32_t dst_clockwise, void* stream) {
+    if (batch < 0) return set_err(HPX_ERR_INVALID_ARG, "negative batch");
+    if (nside < 1 || nside > 8192 || ilog2_exact(nside) < 0)
+        return set_err(HPX_ERR_INVALID_ARG, "nside must be a power of two in [1, 8192]");
+    if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8 && elem_bytes != 16)
+        return set_err(HPX_ERR_INVALID_ARG, "elem_bytes must be 1, 2, 4, 8 or 16");
+    RemapSide src, dst;
+    int rc = remap_side(src_order, src_origin, src_clockwise, &src, "src");
+    if (rc != HPX_OK) return rc;
+    rc = remap_side(dst_order, dst_origin, dst_clockwise, &dst, "dest");
+    if (rc != HPX_OK) return rc;
+    if (batch == 0) return HPX_OK;
+    if (!in || !out) return set_err(HPX_ERR_INVALID_ARG, "null pointer");
+    if ((((uintptr_t)in) | ((uintptr_t)out)) % (uintptr_t)elem_bytes)
+        return set_err(HPX_ERR_INVALID_ARG, "in and out must be aligned to elem_bytes");
+    const uint64_t bytes = (uint64_t)batch * 12ull * nside * nside * (uint64_t)elem_bytes;
+    const uintptr_t a = (uintptr_t)in, b = (uintptr_t)out;
+    if (a < b + bytes && b < a + bytes) return set_err(HPX_ERR_INVALID_ARG, "in and out overlap");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (src.order == dst.order && src.flip == dst.flip && src.rot == dst.rot) {
+        HPX_CUDA_TRY(cudaMemcpyAsync(out, in, bytes, cudaMemcpyDeviceToDevice, st));
+        return HPX_OK;
+    }
+    switch (elem_bytes) {
+        case 1: return launch_remap<uint8_t>(in, out, batch, nside, src, dst, st);
+        case 2: return launch_remap<uint16_t>(in, out, batch, nside, src, dst, st);
+        case 4: return launch_remap<uint32_t>(in, out, batch, nside, src, dst, st);
+        case 8: return launch_remap<unsigned long long>(in, out, batch, nside, src, dst, st);
+        default: return launch_remap<uint4>(in, out, batch, nside, src, dst, st);
+    }
+}
 
 int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream) {
     if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");

@@ -207,6 +207,25 @@ HPX_API int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes);
  * no counterpart in cuHPX. */
 HPX_API int hpx_plan_table_stream_bytes(hpx_plan_t plan, size_t* fwd, size_t* inv);
 
+/* HEALPix pixel-order remapping (no plan needed): batch maps of
+ * 12*nside^2 elements of elem_bytes bytes each (1, 2, 4, 8 or 16; the bytes are
+ * moved, not interpreted), read in the src layout and written in the dst
+ * layout to a separate buffer.  nside is a power of two up to 8192.
+ * Layouts: RING and NEST are HEALPix's; XY ("flat") is face-major with each
+ * face an nside x nside row-major grid whose first pixel sits at the face's
+ * origin corner (S, E, N or W) and whose rows run counter-clockwise, or
+ * clockwise, from it (origin and clockwise are ignored for RING and NEST).
+ * Replaces cuHPX's cuhpx_remap module: ring2nest, nest2ring, nest2xy,
+ * xy2nest, ring2xy, xy2ring, xy2xy and their _batch forms
+ * (src/data_remapping/hpx_remapping.cpp:21-239, 241-450; bound at :452-476;
+ * Python wrappers cuhpx/hpx_remap.py:24-102).  Runs on the stream's device;
+ * allocates nothing; src == dst layouts copy. */
+typedef enum { HPX_ORDER_RING = 0, HPX_ORDER_NEST = 1, HPX_ORDER_XY = 2 } hpx_order_t;
+typedef enum { HPX_ORIGIN_S = 0, HPX_ORIGIN_E = 1, HPX_ORIGIN_N = 2, HPX_ORIGIN_W = 3 } hpx_origin_t;
+HPX_API int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, int32_t elem_bytes,
+                      int32_t src_order, int32_t src_origin, int32_t src_clockwise, int32_t dst_order,
+                      int32_t dst_origin, int32_t dst_clockwise, void* stream);
+
 /* Plan geometry queries. */
 HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);
 
