@@ -1216,9 +1216,9 @@ int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch,
 }
 
 // Opt a remap kernel into more than 48 KB of dynamic shared memory, once per
-// device.
-template <typename K>
-int remap_smem_optin(K kernel, size_t smem) {
+// device and kernel.
+template <auto KERNEL>
+int remap_smem_optin(size_t smem) {
     if (smem <= 48 * 1024) return HPX_OK;
     static std::mutex mu;
     static bool done[64] = {};
@@ -1226,16 +1226,50 @@ int remap_smem_optin(K kernel, size_t smem) {
     HPX_CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mu);
     if (dev < 64 && done[dev]) return HPX_OK;
-    HPX_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (dev < 64) done[dev] = true;
     return HPX_OK;
+}
+
+struct RemapLaunch {
+    dim3 grid;
+    size_t smem;
+    cudaStream_t st;
+    int64_t np;
+    int nside, logs, log_tiles, nb, mpc, vec;
+    RemapSide src, dst;
+};
+
+template <typename E, int SO, int DO>
+int launch_remap_async(const E* in, E* out, const RemapLaunch& L) {
+    const int rc = remap_smem_optin<k_remap_async<E, SO, DO>>(L.smem);
+    if (rc != HPX_OK) return rc;
+    k_remap_async<E, SO, DO><<<L.grid, kRemapThreads, L.smem, L.st>>>(in, out, L.np, L.nside, L.logs, L.log_tiles,
+                                                                      L.nb, L.mpc, L.src, L.dst, L.vec);
+    HPX_CUDA_TRY(cudaGetLastError());
+    return HPX_OK;
+}
+
+template <typename E>
+int dispatch_remap_async(const E* in, E* out, const RemapLaunch& L) {
+    const int so = L.src.order, d = L.dst.order;
+    if (so == kOrderRing && d == kOrderNest) return launch_remap_async<E, kOrderRing, kOrderNest>(in, out, L);
+    if (so == kOrderRing && d == kOrderXY) return launch_remap_async<E, kOrderRing, kOrderXY>(in, out, L);
+    if (so == kOrderNest && d == kOrderRing) return launch_remap_async<E, kOrderNest, kOrderRing>(in, out, L);
+    if (so == kOrderNest && d == kOrderXY) return launch_remap_async<E, kOrderNest, kOrderXY>(in, out, L);
+    if (so == kOrderXY && d == kOrderRing) return launch_remap_async<E, kOrderXY, kOrderRing>(in, out, L);
+    if (so == kOrderXY && d == kOrderNest) return launch_remap_async<E, kOrderXY, kOrderNest>(in, out, L);
+    if (so == kOrderXY && d == kOrderXY) return launch_remap_async<E, kOrderXY, kOrderXY>(in, out, L);
+    return set_err(HPX_ERR_INVALID_ARG, "remap: equal orders are a copy");
 }
 
 // Remap launcher: squares of 64 x 64 pixels for elements of up to 4 bytes and
 // 32 x 32 above, fewer for nside < 64.  Map groups of up to 16 maps a CTA
 // amortise the offsets' arithmetic, while leaving at least 16 CTAs a
-// multiprocessor.  Elements of 4, 8 and 16 bytes take the cp.async pipeline;
-// 1- and 2-byte elements stage through registers.
+// multiprocessor.  Elements of 4, 8 and 16 bytes take the cp.async pipeline
+// (16-byte accesses on NEST and XY sides when the tiles are at least 16 bytes
+// wide and both buffers 16-byte aligned); 1- and 2-byte elements stage
+// through registers.
 template <typename E>
 int launch_remap(const void* in, void* out, int64_t batch, int nside, RemapSide src, RemapSide dst,
                  cudaStream_t st) {
@@ -1250,10 +1284,7 @@ int launch_remap(const void* in, void* out, int64_t batch, int nside, RemapSide 
     constexpr bool kAsync = sizeof(E) >= 4;
     const size_t smem = kAsync ? remap_async_smem_bytes(s, (int)sizeof(E), ring)
                                : remap_smem_bytes(s, (int)sizeof(E), ring);
-    if constexpr (kAsync) {
-        const int rc = remap_smem_optin(k_remap_async<E>, smem);
-        if (rc != HPX_OK) return rc;
-    }
+    const int vec = (s * (int)sizeof(E) >= 16 && ((((uintptr_t)in) | ((uintptr_t)out)) & 15) == 0) ? 1 : 0;
     const int64_t np = 12ll * nside * nside;
     const int64_t chunk = 65535ll * mpc;
     for (int64_t b = 0; b < batch; b += chunk) {
@@ -1262,8 +1293,9 @@ int launch_remap(const void* in, void* out, int64_t batch, int nside, RemapSide 
         const E* pin = (const E*)in + b * np;
         E* pout = (E*)out + b * np;
         if constexpr (kAsync) {
-            k_remap_async<E><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
-                                                                dst);
+            const RemapLaunch L{grid, smem, st, np, nside, logs, log_tiles, nb, mpc, vec, src, dst};
+            const int rc = dispatch_remap_async<E>(pin, pout, L);
+            if (rc != HPX_OK) return rc;
         } else {
             if (s == 64)
                 k_remap<E, 16><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
@@ -1274,8 +1306,8 @@ int launch_remap(const void* in, void* out, int64_t batch, int nside, RemapSide 
             else
                 k_remap<E, 1><<<grid, kRemapThreads, smem, st>>>(pin, pout, np, nside, logs, log_tiles, nb, mpc, src,
                                                                  dst);
+            HPX_CUDA_TRY(cudaGetLastError());
         }
-        HPX_CUDA_TRY(cudaGetLastError());
     }
     return HPX_OK;
 }

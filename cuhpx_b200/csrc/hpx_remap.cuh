@@ -318,14 +318,28 @@ __global__ void __launch_bounds__(kRemapThreads, 5) k_remap(const E* __restrict_
     }
 }
 
-// Elements of 4, 8 or 16 bytes: the same tiles, with the loads issued as
-// cp.async straight into a ring of kRemapStages staged tiles, so that each CTA
-// keeps the next kRemapStages-1 maps' loads in flight the whole time (no
-// registers hold them; 64 x 64 float tiles: three CTAs of 74 KB per SM, 96 KB
-// of loads outstanding) and one barrier per map orders the ring.
+// Elements of 4, 8 or 16 bytes: the same tiles, compiled per (source order,
+// destination order) so that no order test runs per element, with the loads
+// issued as cp.async straight into a ring of kRemapStages staged tiles (each
+// CTA keeps the next kRemapStages-1 maps' loads in flight, and no registers
+// hold them) and one barrier per map ordering the ring.  NEST and XY sides
+// move V = 16 / sizeof(E) consecutive pixels per access (one 16-byte cp.async
+// or store: a NEST tile is one run, an XY tile s rows of s >= V); a RING side
+// moves single elements along its diagonal runs, whose offsets come from the
+// tile's table.  Shared-memory tiles are unpadded: the V-element vectors of
+// each 32-element row are XOR-swizzled by the row number, which keeps every
+// vector 16-byte aligned while spreading transposed and diagonal reads over
+// the banks.  64 x 64 float tiles: 72 KB per CTA, three CTAs and six maps of
+// loads (96 KB) in flight per SM.
 constexpr int kRemapStages = 3;
+
+template <int V>
+HPX_HD int remap_swz(int p) {
+    return p ^ (((p >> 5) & (32 / V - 1)) * V);
+}
 HPX_HD size_t remap_async_smem_bytes(int s, int elem, bool ring) {
-    return kRemapStages * remap_tile_bytes(s, elem) + remap_slot_bytes(s) + (ring ? (size_t)s * s * 4 : 0);
+    return kRemapStages * (((size_t)s * s * elem + 15) & ~(size_t)15) + remap_slot_bytes(s) +
+           (ring ? (size_t)s * s * 4 : 0);
 }
 
 template <int BYTES>
@@ -338,20 +352,52 @@ __device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem) {
         cp_async16(smem, gmem);
 }
 
-template <typename E>
+// offset of natural position p on a NEST or XY side (compile-time order)
+template <int ORDER>
+__device__ __forceinline__ uint32_t nat_offset(uint32_t base, int p, int logs, int nside) {
+    if constexpr (ORDER == kOrderNest) return base + (uint32_t)p;
+    return base + (uint32_t)(p >> logs) * (uint32_t)nside + (uint32_t)(p & ((1 << logs) - 1));
+}
+
+template <typename E, int SO, int DO>
 __global__ void __launch_bounds__(kRemapThreads) k_remap_async(const E* __restrict__ in, E* __restrict__ out,
                                                                int64_t npix, int nside, int logs, int log_tiles,
                                                                int nmaps, int maps_per_cta, RemapSide src,
-                                                               RemapSide dst) {
+                                                               RemapSide dst, int vec) {
     static_assert(sizeof(E) == 4 || sizeof(E) == 8 || sizeof(E) == 16, "cp.async moves 4, 8 or 16 bytes");
+    static_assert(SO != DO || SO == kOrderXY, "equal orders are a copy");
+    constexpr int V = 16 / (int)sizeof(E);
     extern __shared__ __align__(16) unsigned char remap_smem[];
     const int s = 1 << logs, ss = s * s;
-    const size_t tb = remap_tile_bytes(s, (int)sizeof(E));
+    const size_t tb = ((size_t)ss * sizeof(E) + 15) & ~(size_t)15;
     uint16_t* sslot = reinterpret_cast<uint16_t*>(remap_smem + kRemapStages * tb);
     uint32_t* ring_tab = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(sslot) + remap_slot_bytes(s));
+
+    // tile, bases and tables (the slot table holds swizzled source positions)
     Tile t;
-    uint32_t sbase, dbase;
-    remap_setup(t, nside, logs, log_tiles, src, dst, sslot, ring_tab, sbase, dbase);
+    t.s = s;
+    t.logs = logs;
+    t.nside = nside;
+    t.mask = nside - 1;
+    t.f = (int)(blockIdx.x >> (2 * log_tiles));
+    const uint32_t ti = blockIdx.x & ((1u << (2 * log_tiles)) - 1u);
+    t.x0 = (int)compress_bits2(ti) << logs;
+    t.y0 = (int)compress_bits2(ti >> 1) << logs;
+    int sfx = 0, sfy = 0, dfx = 0, dfy = 0;
+    if constexpr (SO == kOrderXY) flat_origin(t, src, sfx, sfy);
+    if constexpr (DO == kOrderXY) flat_origin(t, dst, dfx, dfy);
+    const uint32_t sbase = natural_base(t, src, sfx, sfy);
+    const uint32_t dbase = natural_base(t, dst, dfx, dfy);
+    for (int p = threadIdx.x; p < ss; p += kRemapThreads) {
+        int lx, ly;
+        if constexpr (SO == kOrderRing) {
+            side_coords(t, src, sfx, sfy, p, lx, ly);
+            ring_tab[p] = side_offset(t, src, lx, ly);
+        }
+        side_coords(t, dst, dfx, dfy, p, lx, ly);
+        if constexpr (DO == kOrderRing) ring_tab[p] = side_offset(t, dst, lx, ly);
+        sslot[p] = (uint16_t)remap_swz<V>(side_pos(t, src, sfx, sfy, lx, ly));
+    }
     __syncthreads();
 
     const int b0 = blockIdx.y * maps_per_cta;
@@ -359,8 +405,16 @@ __global__ void __launch_bounds__(kRemapThreads) k_remap_async(const E* __restri
     auto issue = [&](int b) {  // map b -> stage (b - b0) % kRemapStages
         E* tl = reinterpret_cast<E*>(remap_smem + ((b - b0) % kRemapStages) * tb);
         const E* ib = in + (int64_t)b * npix;
-        for (int p = threadIdx.x; p < ss; p += kRemapThreads)
-            cp_async_elem<sizeof(E)>(tl + remap_slot(p), ib + natural_offset(src, sbase, p, logs, nside, ring_tab));
+        if constexpr (SO == kOrderRing) {
+            for (int p = threadIdx.x; p < ss; p += kRemapThreads)
+                cp_async_elem<sizeof(E)>(tl + remap_swz<V>(p), ib + ring_tab[p]);
+        } else if (vec) {
+            for (int p = threadIdx.x * V; p < ss; p += kRemapThreads * V)
+                cp_async16(tl + remap_swz<V>(p), ib + nat_offset<SO>(sbase, p, logs, nside));
+        } else {
+            for (int p = threadIdx.x; p < ss; p += kRemapThreads)
+                cp_async_elem<sizeof(E)>(tl + remap_swz<V>(p), ib + nat_offset<SO>(sbase, p, logs, nside));
+        }
     };
 #pragma unroll
     for (int k = 0; k < kRemapStages - 1; ++k) {
@@ -376,8 +430,22 @@ __global__ void __launch_bounds__(kRemapThreads) k_remap_async(const E* __restri
         cp_async_commit();
         const E* tl = reinterpret_cast<const E*>(remap_smem + ((b - b0) % kRemapStages) * tb);
         E* ob = out + (int64_t)b * npix;
-        for (int p = threadIdx.x; p < ss; p += kRemapThreads)
-            ob[natural_offset(dst, dbase, p, logs, nside, ring_tab)] = tl[sslot[p]];
+        if constexpr (DO == kOrderRing) {
+            for (int p = threadIdx.x; p < ss; p += kRemapThreads) ob[ring_tab[p]] = tl[sslot[p]];
+        } else if (vec) {
+            for (int p = threadIdx.x * V; p < ss; p += kRemapThreads * V) {
+                union {
+                    E e[V];
+                    uint4 w;
+                } u;
+#pragma unroll
+                for (int i = 0; i < V; ++i) u.e[i] = tl[sslot[p + i]];
+                *reinterpret_cast<uint4*>(ob + nat_offset<DO>(dbase, p, logs, nside)) = u.w;
+            }
+        } else {
+            for (int p = threadIdx.x; p < ss; p += kRemapThreads)
+                ob[nat_offset<DO>(dbase, p, logs, nside)] = tl[sslot[p]];
+        }
     }
     cp_async_wait<0>();
 }
