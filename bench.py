@@ -691,6 +691,12 @@ def run_ragged(args):
     return 0
 
 
+# DRAM bytes (read + write) per nside-1024 float32 map of k_remap_async, NEST ->
+# RING, from one ncu capture of an 8-map launch (795.9 MB), scaled by the maps
+# (profiles/remap_nest2ring_nside1024.md)
+REMAP_TRAFFIC_PER_MAP = 795.9e6 / 8
+
+
 def run_remap(args):
     """nest2ring of a batch of float32 maps (default 64 maps at nside 1024,
     3.2 GB each way, larger than L2) per step, the operation the reference's
@@ -773,7 +779,8 @@ def run_remap(args):
         "config": {"workload": f"nest2ring, {B} maps of nside {nside}", "nside": nside, "batch": B,
                    "l2": f"inputs larger than L2 ({byts / 2e9:.2f} GB each way per step)"},
         "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                     "traffic": None, "kernel": "k_remap_async", "peak_source": source, "algorithmic_bytes": byts},
+                     "traffic": REMAP_TRAFFIC_PER_MAP * B if nside == 1024 else None, "kernel": "k_remap_async",
+                     "peak_source": source, "algorithmic_bytes": byts},
         "other_pairs_gbs": {k: byts / (v / args.steps * 1e-3) / 1e9 for k, v in out.items()},
         "e2e": {"value": B * e2e_steps / (e2e_ms * 1e-3), "unit": "maps/s", "h2d_bytes_per_step": npix * 4 * B,
                 "d2h_bytes_per_step": npix * 4 * B, "steps": e2e_steps},
