@@ -692,8 +692,8 @@ def run_ragged(args):
 
 
 # DRAM bytes (read + write) per nside-1024 float32 map of k_remap_async, NEST ->
-# RING, from one ncu capture of an 8-map launch (795.9 MB), scaled by the maps
-# (profiles/remap_nest2ring_nside1024.md)
+# RING, from one ncu capture of an 8-map launch (795.9 MB: dram__bytes_read.sum
+# + dram__bytes_write.sum), scaled by the maps
 REMAP_TRAFFIC_PER_MAP = 795.9e6 / 8
 
 
