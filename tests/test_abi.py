@@ -97,3 +97,30 @@ def test_no_gpu_is_a_status_not_a_crash(lib):
     h = ctypes.c_void_p()
     st = lib.hpx_plan_create(ctypes.byref(_desc()), ctypes.byref(h))
     assert st == 3 and not h.value
+
+
+def test_remap_rejects_bad_arguments_before_any_cuda_call(lib):
+    """hpx_remap validates everything on the host first; none of these reaches the GPU."""
+    RING, NEST, XY = 0, 1, 2
+    a, b = ctypes.c_void_p(0x10000), ctypes.c_void_p(0x90000000)
+
+    def call(inp=a, out=b, batch=1, nside=4, elem=4, so=NEST, sorg=0, scw=0, do=RING, dorg=0, dcw=0):
+        return lib.hpx_remap(inp, out, batch, nside, elem, so, sorg, scw, do, dorg, dcw, None)
+
+    assert call(batch=0) == 0  # nothing to do
+    assert call(batch=-1) == 1
+    for bad in (0, 3, 12, 16384):
+        assert call(nside=bad) == 1
+    assert b"power of two" in lib.hpx_last_error(None)
+    for bad in (0, 3, 32):
+        assert call(elem=bad) == 1
+    assert call(so=3) == 1
+    assert call(so=XY, sorg=4) == 1
+    assert b"src origin" in lib.hpx_last_error(None)
+    assert call(do=XY, dorg=-1) == 1
+    assert b"dest origin" in lib.hpx_last_error(None)
+    assert call(inp=ctypes.c_void_p(0)) == 1
+    assert call(inp=ctypes.c_void_p(0x10002)) == 1  # not 4-byte aligned
+    assert b"aligned" in lib.hpx_last_error(None)
+    assert call(out=ctypes.c_void_p(0x10000 + 64)) == 1  # overlapping buffers
+    assert b"overlap" in lib.hpx_last_error(None)
