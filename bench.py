@@ -7,7 +7,7 @@ white noise, generated on the device from a fixed seed; each batch is 3.2 GB,
 larger than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N --steps K --warmup W] [--precision f16x3|bf16x3|fp32] [--refine k]
-  python bench.py --impl reference ...   # the reference's CPU algorithm (oracle port) on the host
+  python bench.py --impl reference ...   # the reference's CPU algorithm (multi-threaded port) on the host
 
 Under torchrun every rank runs its own batch (replicas, no collective on the
 data path); the timed region is bracketed by barriers and the max over ranks
@@ -52,8 +52,8 @@ def parse():
     ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged", "remap"],
                     help="sht_isht: the headline step; ragged: 96 maps of mixed nside; remap: NEST -> RING "
                          "reordering of a batch of maps (with the other layout pairs beside it)")
-    ap.add_argument("--accuracy-maps", type=int, default=2)
-    ap.add_argument("--cpu-sample-m", type=int, default=12)
+    ap.add_argument("--accuracy-maps", type=int, default=16)
+    ap.add_argument("--spot-maps", type=int, default=2, help="maps checked against the CPU spot oracle")
     return ap.parse_args()
 
 
@@ -118,44 +118,75 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU baseline
-def cpu_baseline(nside, lmax, n_m, steps=1):
-    from oracle import hpx_oracle as O
+def host_info():
+    """CPU model, logical cores and RAM of this host (for the CPU timings)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    ram = None
+    try:
+        ram = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30
+    except (ValueError, OSError):
+        pass
+    return {"cpu_model": model, "logical_cores": os.cpu_count(), "ram_gib": ram}
 
-    cores = os.cpu_count() or 1
-    secs = []
-    for s in range(steps):
-        r = O.time_reference_sample(nside, lmax, lmax, n_m=n_m, seed=s, threads=cores)
-        secs.append(r["seconds_per_map"])
+
+def _ref_port(threads=None):
+    """The multi-threaded CPU port of the reference's SHT/iSHT (oracle/ref_cpu)."""
+    from oracle import ref_cpu as RC
+
+    RC.load()
+    if threads:
+        RC.set_threads(threads)
+    return RC
+
+
+PORT_SAMPLE = ("per map: the reference's CPU SHT then iSHT (cuhpx/hpx_sht.py:173-283) in float64 -- one rfft/irfft "
+               "per ring (numpy) and the Legendre contraction over every order m < M and degree m <= l < L (C, "
+               "OpenMP over the orders, the table's values regenerated per order by the reference's recurrence "
+               "instead of held: 68.6 GB at nside 1024)")
+
+
+def cpu_baseline(nside, lmax, min_seconds=10.0):
+    """The CPU port timed on whole maps (all orders) for at least min_seconds."""
+    RC = _ref_port(os.cpu_count())
+    RC.time_sht_isht(nside, lmax, lmax, seed=99)  # warm-up (page-in, thread pool)
+    secs, t0 = [], time.perf_counter()
+    while len(secs) < 2 or time.perf_counter() - t0 < min_seconds:
+        secs.append(RC.time_sht_isht(nside, lmax, lmax, seed=len(secs)))
     spm = statistics.median(secs)
     return {
         "value": 1.0 / spm,
         "unit": "maps/s",
-        "cores": cores,
+        "cores": RC.threads(),
         "kind": "port",
-        "sample": (
-            f"one float64 map at nside={nside}, L=M={lmax}: all ring rfft/irfft, and the reference's dense per-m "
-            f"Legendre contraction timed on {r['n_m']} sampled orders and scaled by M/{r['n_m']} (the full dense "
-            f"table is 68.6 GB); numpy with {cores} host threads"
-        ),
+        "sample": f"{len(secs)} maps at nside={nside}, L=M={lmax}, one at a time; " + PORT_SAMPLE,
         "seconds_per_map": spm,
+        "host": host_info(),
     }
 
 
 def run_reference(args):
+    """The reference's CPU implementation (its port, every order) on the host:
+    each step is one whole float64 map, SHT then iSHT, timed end to end."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     lm = args.lmax
-    cores = os.cpu_count() or 1
-    from oracle import hpx_oracle as O
-
+    RC = _ref_port(os.cpu_count())
+    cores = RC.threads()
     for w in range(args.warmup):
-        O.time_reference_sample(args.nside, lm, lm, n_m=max(2, args.cpu_sample_m // 4), seed=100 + w, threads=cores)
-    secs = []
+        RC.time_sht_isht(args.nside, lm, lm, seed=100 + w)
+    t0 = time.perf_counter()
     for s in range(args.steps):
-        r = O.time_reference_sample(args.nside, lm, lm, n_m=args.cpu_sample_m, seed=s, threads=cores)
-        secs.append(r["seconds_per_map"])
-    total = sum(secs)
+        RC.time_sht_isht(args.nside, lm, lm, seed=s)
+    total = time.perf_counter() - t0
     value = args.steps / total
     line = {
         "impl": "reference",
@@ -171,14 +202,17 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"SHT+iSHT nside={args.nside} lmax=mmax={lm}, one map per step (bounded sample)", "batch": 1},
+        "config": {"workload": f"SHT+iSHT nside={args.nside} lmax=mmax={lm}, one whole map per step (a bounded "
+                               f"sample of the batch of {args.batch})", "batch": 1, "nside": args.nside, "lmax": lm,
+                   "mmax": lm},
         "cpu_baseline": {
             "value": value,
             "unit": "maps/s",
             "cores": cores,
             "kind": "port",
-            "sample": f"per step one map: full ring FFTs + dense per-m Legendre contraction on {args.cpu_sample_m} sampled orders scaled by M",
+            "sample": "one map per step, every order and degree computed; " + PORT_SAMPLE,
         },
+        "host": host_info(),
         "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -265,7 +299,13 @@ def run_gpu(args):
             a = sht(f)
             out["f2"] = isht(a)
 
+    # plan creation (ring tables, Legendre seeds, chirp spectra and, for
+    # tensor-core plans, the resident Legendre table) timed on its own
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter()
     plan = hpx.get_plan(nside, L, L, "ring", prec, local)
+    torch.cuda.synchronize()
+    plan_create_s = time.perf_counter() - t_plan
     clocks = ClockSampler(local)
     # warm-up, then the timed region with per-kernel events and clock sampling
     for _ in range(args.warmup):
@@ -329,7 +369,7 @@ def run_gpu(args):
 
     acc = None
     if not args.no_accuracy:
-        acc = accuracy_vs_fp64(torch, hpx, sht, isht, f[: args.accuracy_maps], nside, L, refine)
+        acc = accuracy_vs_fp64(torch, hpx, sht, isht, f[: args.accuracy_maps], nside, L, refine, args.spot_maps)
 
     # the workload's refined variants: k Jacobi iterations in the analysis (each
     # one more synthesis and analysis of the residual), the same maps, and their
@@ -357,7 +397,7 @@ def run_gpu(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(nside, L, args.cpu_sample_m)
+        cpu = cpu_baseline(nside, L)
 
     if rank == 0:
         line = {
@@ -385,6 +425,7 @@ def run_gpu(args):
                 "parallelism": f"replicas x{world}",
             },
             "gpu_launches": int(round(launches_per_step * args.steps)),
+            "plan": {"create_s": plan_create_s, "table_bytes": plan.table_bytes},
             "kernels_per_step": launches_per_step,
             "stage_ms_per_step": {k: v[1] / args.steps for k, v in stats.items() if v[0]},
             "roofline": roof,
@@ -403,10 +444,13 @@ def run_gpu(args):
     return 0
 
 
-def accuracy_vs_fp64(torch, hpx, sht, isht, f, nside, L, refine):
+def accuracy_vs_fp64(torch, hpx, sht, isht, f, nside, L, refine, spot_maps=0):
     """Rel-L2 of the timed modules against the FP64 path with the same Jacobi
-    iterations, on a few of the timed maps: the analysis coefficients and the
-    round trip iSHT(SHT(f))."""
+    iterations, on the first maps of the timed batch: the analysis coefficients
+    and the round trip iSHT(SHT(f)).  With spot_maps > 0 (no refinement), the
+    orders 0, 1, 2, M/4, M/2 and M-1 of the first spot_maps maps are also
+    compared with the CPU spot oracle (one float64 Legendre column at a time,
+    oracle/hpx_oracle.py sht_spot), for the timed path and the FP64 path."""
 
     def rel(a, b):
         return float((a.to(b.dtype) - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt())
@@ -423,8 +467,23 @@ def accuracy_vs_fp64(torch, hpx, sht, isht, f, nside, L, refine):
             "alm_rel_l2": rel(a, a64),
             "roundtrip_rel_l2": rel(r, r64),
             "tolerance": 1e-5,
-            "reference": "this library's FP64 path (FP64 FFTs, FP64 Legendre recurrence and contraction), same refine_iters",
+            "reference": "this library's FP64 path (FP64 FFTs, FP64 Legendre recurrence and contraction), same "
+                         "refine_iters",
         }
+        if spot_maps > 0 and refine == 0:
+            from oracle import hpx_oracle as O
+
+            ms = sorted({0, 1, 2, L // 4, L // 2, L - 1})
+            ref = O.sht_spot(f64[:spot_maps].cpu().numpy(), nside, L, L, ms)
+            ref_t = torch.from_numpy(ref).to(a.device)
+            out["spot_oracle"] = {
+                "maps": spot_maps,
+                "orders": ms,
+                "alm_rel_l2": rel(a[:spot_maps, :, ms], ref_t),
+                "fp64_path_alm_rel_l2": rel(a64[:spot_maps, :, ms], ref_t),
+                "reference": "CPU float64 spot oracle: ring rfft + one Legendre column per order by the "
+                             "reference's recurrence (cuhpx/hpx_sht.py:214-236, cuhpx/sht_tools.py:204-214)",
+            }
         del f64, a64, r64
     torch.cuda.empty_cache()
     return out

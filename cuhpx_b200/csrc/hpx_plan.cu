@@ -1177,23 +1177,60 @@ namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct NoAllocSlot {
+    unsigned long long ctx_id = 0;  // driver context ID the address belongs to (0: none yet)
+    void* ptr = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
 
-// Address of the scratch on `device`, looked up once per device with that
-// device current (the caller holds a DeviceGuard for it).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// ID of the current context, unique for the life of the process (a context
+// created after cudaDeviceReset gets a new one); 0 when it cannot be read.
+unsigned long long current_ctx_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)fn;
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)fn;
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur && get_id && get_cur(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
+
+// Address of the scratch on `device` (the caller holds a DeviceGuard for it):
+// looked up with cudaGetSymbolAddress on the first call on the device, and
+// again whenever the device's context is not the one the cached address
+// belongs to (after cudaDeviceReset the array lives at a new address).
 int noalloc_scratch(int device, unsigned char** out) {
     if (device < 0 || device >= kNoAllocMaxDevices) return set_err(HPX_ERR_UNSUPPORTED, "device ordinal above 63");
+    const unsigned long long id = current_ctx_id();
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_ptr[device]) {
+    NoAllocSlot& slot = g_noalloc_slot[device];
+    if (!slot.ptr || id == 0 || slot.ctx_id != id) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             cudaGetLastError();
+            slot = NoAllocSlot{};
             return set_err(HPX_ERR_CUDA, std::string("scratch symbol address: ") + cudaGetErrorString(e));
         }
-        g_noalloc_ptr[device] = p;
+        slot.ptr = p;
+        slot.ctx_id = id;
     }
-    *out = (unsigned char*)g_noalloc_ptr[device];
+    *out = (unsigned char*)slot.ptr;
     return HPX_OK;
 }
 
@@ -1351,7 +1388,11 @@ int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, int32_t e
     if (!in || !out) return set_err(HPX_ERR_INVALID_ARG, "null pointer");
     if ((((uintptr_t)in) | ((uintptr_t)out)) % (uintptr_t)elem_bytes)
         return set_err(HPX_ERR_INVALID_ARG, "in and out must be aligned to elem_bytes");
-    const uint64_t bytes = (uint64_t)batch * 12ull * nside * nside * (uint64_t)elem_bytes;
+    // bytes of one batch, bounded by 2^62 so that neither the product nor the
+    // overlap test's sums (user addresses are below 2^57) can wrap
+    const uint64_t per_map = 12ull * (uint64_t)nside * (uint64_t)nside * (uint64_t)elem_bytes;
+    if ((uint64_t)batch > (1ull << 62) / per_map) return set_err(HPX_ERR_INVALID_ARG, "batch too large");
+    const uint64_t bytes = (uint64_t)batch * per_map;
     const uintptr_t a = (uintptr_t)in, b = (uintptr_t)out;
     if (a < b + bytes && b < a + bytes) return set_err(HPX_ERR_INVALID_ARG, "in and out overlap");
     cudaStream_t st = (cudaStream_t)stream;

@@ -86,4 +86,10 @@ def main(src_dir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/cuhpx/data")
+    # the FITS folder of a cuHPX checkout: first argument, or $CUHPX_REFERENCE/cuhpx/data
+    src = sys.argv[1] if len(sys.argv) > 1 else None
+    if src is None and os.environ.get("CUHPX_REFERENCE"):
+        src = os.path.join(os.environ["CUHPX_REFERENCE"], "cuhpx", "data")
+    if src is None:
+        sys.exit("usage: make_ring_weights.py <cuHPX>/cuhpx/data  (or set CUHPX_REFERENCE)")
+    main(src)

@@ -133,7 +133,9 @@ HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void*
  * at zero.  Calls that overlap in time -- on two streams, or from two threads --
  * race on the array and give wrong results: serialise them.  The first call on
  * a device looks up the array's address (cudaGetSymbolAddress, with the plan's
- * device current); make that first call before any stream capture. */
+ * device current); make that first call before any stream capture.  The
+ * address belongs to the device's context: after cudaDeviceReset the next call
+ * looks it up again (make that call outside stream capture too). */
 HPX_API int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream);
 
 /* Ragged batches: n_groups groups of maps, group g with its own plan (for

@@ -10,7 +10,7 @@ repository to a GPU machine, where ``tests/test_remap_gpu.py`` runs the
 reference's kernels beside this library's and requires identical output.
 Nothing in the product imports it.
 
-    python -m oracle.build_ref_remap [--reference /path/to/cuHPX]
+    python -m oracle.build_ref_remap --reference /path/to/cuHPX   (or set CUHPX_REFERENCE)
 """
 
 import argparse
@@ -18,7 +18,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+# a cuHPX checkout; the build is skipped when none is given
+DEFAULT_REFERENCE = os.environ.get("CUHPX_REFERENCE")
 SOURCES = ["src/data_remapping/hpx_remapping.cpp", "src/data_remapping/hpx_remapping_cuda.cu"]
 
 
@@ -27,6 +28,8 @@ def built_path():
 
 
 def build(reference=DEFAULT_REFERENCE, verbose=False):
+    if not reference:
+        return None
     srcs = [os.path.join(reference, s) for s in SOURCES]
     if not all(os.path.exists(s) for s in srcs):
         return None  # no reference checkout on this machine: keep any prebuilt copy

@@ -304,6 +304,29 @@ def sht_spot(f, nside, lmax, mmax, ms, quad_weights="ring"):
     return out
 
 
+def sht_by_m(f, nside, lmax, mmax, quad_weights="ring"):
+    """``sht`` computed one order at a time (all columns of ``sht_spot``).
+
+    Same values as ``sht`` (the Legendre columns come from the same
+    recurrence); O(lmax * rings) Legendre memory and matrix products per
+    order, so it finishes in seconds at nside 256, L = M = 511.
+    """
+    return sht_spot(f, nside, lmax, mmax, list(range(mmax)), quad_weights)
+
+
+def isht_by_m(alm, nside):
+    """``isht`` computed one order at a time (cuhpx/hpx_sht.py:268-283): the
+    ring spectra of order m are the Legendre column of m applied to a[..., :, m]."""
+    alm = np.asarray(alm, dtype=np.complex128)
+    L, M = alm.shape[-2], alm.shape[-1]
+    x = np.cos(ring_theta(nside))
+    ftm = np.zeros(alm.shape[:-2] + (x.size, M), dtype=np.complex128)
+    for m in range(min(M, L)):
+        P = legendre_column(m, L, x)  # [L, R]
+        ftm[..., :, m] = np.einsum("...l,lt->...t", alm[..., :, m], P)
+    return ring_irfft(ftm, M, nside)
+
+
 # --------------------------------------------------------------------------- CPU baseline timing
 def time_reference_sample(nside, lmax, mmax, n_m=8, seed=0, threads=None):
     """Time the reference CPU algorithm on one map, sampling the Legendre stage.

@@ -2,9 +2,9 @@
 
 Runs the reference's own CPU transforms (``cuhpx.SHT`` / ``cuhpx.iSHT``,
 cuhpx/hpx_sht.py:173-283, loaded by ``ref_loader.py``) on seeded inputs and
-stores inputs and outputs.  Needs the cuHPX sources (default
-``/root/reference``); the fixtures it writes are committed so that nothing
-else needs them.
+stores inputs and outputs.  Needs the cuHPX sources (first argument, or the
+``CUHPX_REFERENCE`` environment variable); the fixtures it writes are
+committed so that nothing else needs them.
 
 Cases (each an ``.npz``):
   cfg1_n32     nside=32, L=M=65, one N(0,1) map (seed 0), 'ring' weights:
@@ -53,7 +53,7 @@ def run(hpx_sht, nside, L, M, f64, qw="ring"):
     )
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
     hpx_sht, _ = load_reference(ref_root)
     torch.set_num_threads(os.cpu_count() or 1)
 

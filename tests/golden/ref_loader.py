@@ -60,8 +60,15 @@ def _fits_shim():
     sys.modules.setdefault("astropy.io.fits", fits)
 
 
-def load_reference(ref_root="/root/reference"):
-    """Return the reference ``cuhpx.hpx_sht`` module (CPU classes usable)."""
+def load_reference(ref_root=None):
+    """Return the reference ``cuhpx.hpx_sht`` module (CPU classes usable).
+
+    ``ref_root`` is a cuHPX checkout; by default the ``CUHPX_REFERENCE``
+    environment variable names it.
+    """
+    ref_root = ref_root or os.environ.get("CUHPX_REFERENCE")
+    if not ref_root:
+        raise FileNotFoundError("no cuHPX checkout given (argument or CUHPX_REFERENCE)")
     pkg_dir = os.path.join(ref_root, "cuhpx")
     if not os.path.isdir(pkg_dir):
         raise FileNotFoundError(f"cuHPX sources not found at {pkg_dir}")

@@ -124,3 +124,6 @@ def test_remap_rejects_bad_arguments_before_any_cuda_call(lib):
     assert b"aligned" in lib.hpx_last_error(None)
     assert call(out=ctypes.c_void_p(0x10000 + 64)) == 1  # overlapping buffers
     assert b"overlap" in lib.hpx_last_error(None)
+    # a byte count that would wrap 64 bits is refused before the overlap test
+    assert call(batch=2**62, nside=8192, elem=16) == 1
+    assert b"batch too large" in lib.hpx_last_error(None)

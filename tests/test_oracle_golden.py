@@ -106,3 +106,43 @@ def test_weights_sum_to_sphere_area():
         nphi = np.array([O.nphi_ring(t, nside) for t in range(O.nrings(nside))])
         # pixel-weighted sum of the quadrature weights integrates 1 over the sphere
         assert abs((w * nphi).sum() / (4 * np.pi) - 1) < 5e-3
+
+
+@pytest.mark.parametrize("name,L,M", [("cfg1_n32.npz", 65, 65), ("lm_n8.npz", 9, 17), ("lm_n8.npz", 17, 5)])
+def test_per_order_oracle_matches_full(name, L, M):
+    # the per-order transforms (used where the full ones would take minutes)
+    # give the golden-pinned values
+    d = load(name)
+    nside = 32 if name.startswith("cfg1") else 8
+    f = d["f"] if "f" in d.files else d["mgt_f"]
+    a = O.sht(f, nside, L, M)
+    assert rel(O.sht_by_m(f, nside, L, M), a) < 1e-14
+    assert rel(O.isht_by_m(a, nside), O.isht(a, nside)) < 1e-14
+
+
+@pytest.fixture(scope="module")
+def ref_cpu():
+    from oracle import ref_cpu as RC
+
+    try:
+        RC.load()
+    except Exception as e:  # no C compiler with OpenMP on this machine
+        pytest.skip(f"ref_cpu not built: {e}")
+    return RC
+
+
+@pytest.mark.parametrize("nside,L,M", [(8, 17, 17), (8, 9, 17), (8, 17, 5), (16, 33, 33), (32, 65, 65)])
+def test_cpu_baseline_port_matches_oracle(ref_cpu, nside, L, M):
+    # the multi-threaded C port that bench.py times as the reference's CPU
+    # implementation computes the oracle's transforms
+    rng = np.random.default_rng(nside + L + M)
+    f = rng.standard_normal(12 * nside * nside)
+    a = O.sht(f, nside, L, M)
+    assert rel(ref_cpu.sht(f, nside, L, M), a) < 1e-13
+    assert rel(ref_cpu.isht(a, nside), O.isht(a, nside)) < 1e-13
+
+
+def test_cpu_baseline_port_matches_reference_goldens(ref_cpu):
+    d = load("cfg1_n32.npz")
+    assert rel(ref_cpu.sht(d["f"], 32, 65, 65), d["alm64"]) < 1e-7
+    assert rel(ref_cpu.isht(d["alm64"], 32), d["map64"]) < 1e-7

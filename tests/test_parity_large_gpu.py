@@ -1,0 +1,150 @@
+"""Parity with the CPU oracle at the survey's large configurations.
+
+cfg2: synthesis -> analysis round trip at nside 256, L = M = 511, 8 maps whose
+a_lm are complex Gaussian with variance C_l ~ (l+1)^-2 (m <= l, Im a_l0 = 0),
+against the full float64 oracle (its per-order form, pinned to the full
+transforms on the CPU).  Bars (rel-L2):
+  FP64 path                       <= 1e-10
+  plain FP32 path                 <= 1e-5
+  f16x3 / bf16x3 with 1 Jacobi iteration vs the oracle with 1 iteration <= 1e-5
+  f16x3 / bf16x3 synthesis        <= 1e-5
+
+cfg3: nside 1024, L = M = 2047, maps of the benchmark's recipe (band-limited
+field plus N(0, 1e-3) noise):
+  * spot oracle (orders 0, 1, 2, 511, 1023, 2046; one Legendre column at a
+    time) on 2 maps: FP64 path <= 1e-10, FP32 and f16x3 <= 1e-5;
+  * the whole coefficient set of one map against the multi-threaded port of
+    the reference's CPU transform (oracle/ref_cpu.c, pinned to the oracle on
+    the CPU): FP64 <= 1e-10, FP32 <= 1e-5, f16x3 with 1 Jacobi iteration vs
+    the port with 1 iteration <= 1e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import hpx_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = a.detach().cpu().numpy() if torch.is_tensor(a) else np.asarray(a)
+    b = b.detach().cpu().numpy() if torch.is_tensor(b) else np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def cl_alm(rng, L, batch):
+    """complex Gaussian a_lm with variance (l+1)^-2, m <= l, Im a_l0 = 0"""
+    sig = 1.0 / (np.arange(L) + 1.0)[:, None]
+    a = (rng.standard_normal((batch, L, L)) + 1j * rng.standard_normal((batch, L, L))) * sig / np.sqrt(2.0)
+    a = np.where(np.arange(L)[None, :] <= np.arange(L)[:, None], a, 0)
+    a[..., 0] = a[..., 0].real
+    return a
+
+
+@pytest.fixture(scope="module")
+def hpx(cuda):
+    import cuhpx_b200
+
+    return cuhpx_b200
+
+
+# --------------------------------------------------------------------------- cfg2
+N2, L2, B2 = 256, 511, 8
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    rng = np.random.default_rng(1)
+    a = cl_alm(rng, L2, B2)
+    f = O.isht_by_m(a, N2)  # band-limited maps
+    a0 = O.sht_by_m(f, N2, L2, L2)
+    # one Jacobi iteration in float64: a1 = a0 + SHT(f - iSHT(a0))
+    a1 = a0 + O.sht_by_m(f - O.isht_by_m(a0, N2), N2, L2, L2)
+    return dict(a=a, f=f, a0=a0, a1=a1)
+
+
+def test_cfg2_fp64(hpx, cuda, cfg2):
+    sht = hpx.SHTCUDA(N2, lmax=L2, mmax=L2)
+    isht = hpx.iSHTCUDA(N2, lmax=L2, mmax=L2)
+    assert rel(isht(torch.from_numpy(cfg2["a"]).to(cuda)), cfg2["f"]) < 1e-10
+    assert rel(sht(torch.from_numpy(cfg2["f"]).to(cuda)), cfg2["a0"]) < 1e-10
+
+
+def test_cfg2_plain_fp32(hpx, cuda, cfg2):
+    sht = hpx.SHTCUDA(N2, lmax=L2, mmax=L2, precision="fp32")
+    isht = hpx.iSHTCUDA(N2, lmax=L2, mmax=L2, precision="fp32")
+    assert rel(isht(torch.from_numpy(cfg2["a"]).to(cuda, torch.complex64)), cfg2["f"]) < 1e-5
+    assert rel(sht(torch.from_numpy(cfg2["f"]).to(cuda, torch.float32)), cfg2["a0"]) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["f16x3", "bf16x3"])
+def test_cfg2_mixed(hpx, cuda, cfg2, prec):
+    f32 = torch.from_numpy(cfg2["f"]).to(cuda, torch.float32)
+    isht = hpx.iSHTCUDA(N2, lmax=L2, mmax=L2, precision=prec)
+    assert rel(isht(torch.from_numpy(cfg2["a"]).to(cuda, torch.complex64)), cfg2["f"]) < 1e-5
+    sht1 = hpx.SHTCUDA(N2, lmax=L2, mmax=L2, precision=prec, refine_iters=1)
+    assert rel(sht1(f32), cfg2["a1"]) < 1e-5
+    # without refinement the error is reported, not bounded by 1e-5; keep it in its known range
+    sht0 = hpx.SHTCUDA(N2, lmax=L2, mmax=L2, precision=prec, refine_iters=0)
+    assert rel(sht0(f32), cfg2["a0"]) < 3e-5
+
+
+# --------------------------------------------------------------------------- cfg3
+N3, L3 = 1024, 2047
+SPOT = [0, 1, 2, 511, 1023, 2046]
+
+
+@pytest.fixture(scope="module")
+def cfg3_maps(hpx, cuda):
+    """2 maps of the benchmark recipe, synthesised on the device in FP64."""
+    rng = np.random.default_rng(3)
+    a = torch.from_numpy(cl_alm(rng, L3, 2)).to(cuda)
+    with torch.no_grad():
+        f = hpx.iSHTCUDA(N3, lmax=L3, mmax=L3)(a)
+    del a
+    f = f.cpu().numpy() + rng.standard_normal(f.shape) * np.sqrt(1e-3)
+    torch.cuda.empty_cache()
+    return f
+
+
+def test_cfg3_spot_oracle(hpx, cuda, cfg3_maps):
+    f = cfg3_maps
+    ref = O.sht_spot(f, N3, L3, L3, SPOT)
+    x = torch.from_numpy(f).to(cuda)
+    with torch.no_grad():
+        a64 = hpx.SHTCUDA(N3, lmax=L3, mmax=L3)(x)[..., SPOT]
+        assert rel(a64, ref) < 1e-10
+        a32 = hpx.SHTCUDA(N3, lmax=L3, mmax=L3, precision="fp32")(x.float())[..., SPOT]
+        assert rel(a32, ref) < 1e-5
+        amx = hpx.SHTCUDA(N3, lmax=L3, mmax=L3, precision="f16x3", refine_iters=0)(x.float())[..., SPOT]
+        assert rel(amx, ref) < 1e-5
+    torch.cuda.empty_cache()
+
+
+@pytest.fixture(scope="module")
+def ref_cpu():
+    from oracle import ref_cpu as RC
+
+    try:
+        RC.load()
+    except Exception as e:
+        pytest.skip(f"CPU port not built: {e}")
+    return RC
+
+
+def test_cfg3_full_vs_cpu_port(hpx, cuda, cfg3_maps, ref_cpu):
+    f = cfg3_maps[0]
+    a0 = ref_cpu.sht(f, N3, L3, L3)
+    a1 = a0 + ref_cpu.sht(f - ref_cpu.isht(a0, N3), N3, L3, L3)
+    x = torch.from_numpy(f).to(cuda)
+    with torch.no_grad():
+        assert rel(hpx.SHTCUDA(N3, lmax=L3, mmax=L3)(x), a0) < 1e-10
+        assert rel(hpx.SHTCUDA(N3, lmax=L3, mmax=L3, precision="fp32")(x.float()), a0) < 1e-5
+        got = hpx.SHTCUDA(N3, lmax=L3, mmax=L3, precision="f16x3", refine_iters=1)(x.float())
+        assert rel(got, a1) < 1e-5
+        # synthesis of the FP64 coefficients
+        g = hpx.iSHTCUDA(N3, lmax=L3, mmax=L3, precision="f16x3")(torch.from_numpy(a0).to(cuda, torch.complex64))
+        assert rel(g, ref_cpu.isht(a0, N3)) < 1e-5
+    torch.cuda.empty_cache()

@@ -82,6 +82,38 @@ def test_noalloc_matches_forward_twice(lib, cuda, nside, L, M, prec, batch):
         lib.hpx_plan_destroy(plan)
 
 
+def make_latlon_plan(lib, nlat, nlon, L, M, precision, grid=0):
+    d = _lib.HpxLatLonDesc()
+    d.nlat, d.nlon, d.lmax, d.mmax, d.grid, d.precision = nlat, nlon, L, M, grid, precision
+    d.batch_chunk, d.device, d.flags, d.reserved = 0, 0, 0, 0
+    h = ctypes.c_void_p()
+    _lib.check(lib.hpx_plan_create_latlon(ctypes.byref(d), ctypes.byref(h)))
+    return h
+
+
+# latitude-longitude plans take the same scratch layout: (nlat, nlon, L, M, precision, batch, grid)
+LATLON = [(32, 64, 32, 32, 0, 5, 0), (32, 64, 32, 32, 2, 70, 0), (33, 64, 30, 20, 4, 3, 1)]
+
+
+@pytest.mark.parametrize("nlat,nlon,L,M,prec,batch,grid", LATLON)
+def test_noalloc_latlon_matches_forward_twice(lib, cuda, nlat, nlon, L, M, prec, batch, grid):
+    plan = make_latlon_plan(lib, nlat, nlon, L, M, prec, grid)
+    try:
+        stream = torch.cuda.current_stream(cuda).cuda_stream
+        g = torch.Generator(device="cpu").manual_seed(nlat * 100 + prec)
+        for _ in range(2):
+            f = torch.randn(batch, nlat * nlon, generator=g).to(cuda)
+            ref = torch.empty(batch, L, M, 2, device=cuda)
+            forward_ws(lib, plan, f, ref, stream)
+            out = torch.full((batch, L, M, 2), float("nan"), device=cuda)
+            _lib.check(lib.hpx_sht_forward_noalloc(plan, f.data_ptr(), out.data_ptr(), batch, stream), plan)
+            _lib.check(lib.hpx_plan_check(plan, stream), plan)
+            torch.cuda.synchronize()
+            assert torch.equal(out, ref), float((out - ref).abs().max())
+    finally:
+        lib.hpx_plan_destroy(plan)
+
+
 def test_noalloc_refuses_plans_above_scratch(lib, cuda):
     # FP32, nside 64, lmax = mmax = 192: about 36 MiB per chunk of 64 maps
     plan = make_plan(lib, 64, 192, 192, 0)
