@@ -474,15 +474,20 @@ def accuracy_vs_fp64(torch, hpx, sht, isht, f, nside, L, refine, spot_maps=0):
             from oracle import hpx_oracle as O
 
             ms = sorted({0, 1, 2, L // 4, L // 2, L - 1})
-            ref = O.sht_spot(f64[:spot_maps].cpu().numpy(), nside, L, L, ms)
-            ref_t = torch.from_numpy(ref).to(a.device)
+            fs = f64[:spot_maps].cpu().numpy()
+            ex = torch.from_numpy(O.sht_spot(fs, nside, L, L, ms, nodes="exact")).to(a.device)
+            rf = torch.from_numpy(O.sht_spot(fs, nside, L, L, ms)).to(a.device)
             out["spot_oracle"] = {
                 "maps": spot_maps,
                 "orders": ms,
-                "alm_rel_l2": rel(a[:spot_maps, :, ms], ref_t),
-                "fp64_path_alm_rel_l2": rel(a64[:spot_maps, :, ms], ref_t),
-                "reference": "CPU float64 spot oracle: ring rfft + one Legendre column per order by the "
-                             "reference's recurrence (cuhpx/hpx_sht.py:214-236, cuhpx/sht_tools.py:204-214)",
+                "alm_rel_l2": rel(a[:spot_maps, :, ms], ex),
+                "fp64_path_alm_rel_l2": rel(a64[:spot_maps, :, ms], ex),
+                "reference_form_alm_rel_l2": rel(rf, ex),
+                "reference": "CPU spot oracle: float64 ring rfft + one Legendre column per order by the "
+                             "reference's recurrence (cuhpx/hpx_sht.py:214-236, cuhpx/sht_tools.py:204-214) in "
+                             "80-bit extended precision at the plan's ring nodes; reference_form_alm_rel_l2 is the "
+                             "reference's own FP64 recurrence against it (its diagonal goes subnormal for high "
+                             "orders near the poles)",
             }
         del f64, a64, r64
     torch.cuda.empty_cache()

@@ -90,6 +90,17 @@ def ring_z(nside):
     return z
 
 
+def ring_sin2(nside):
+    """sin^2(theta) of every ring from the z formula without cancellation near
+    the poles: a (2 - a) with a = 1 - |z| = (t+1)^2 / (3 nside^2) on the polar
+    rings, (1 - z)(1 + z) elsewhere (the "exact" nodes of ``sht_spot``)."""
+    t = np.arange(4 * nside - 1)
+    tn = np.where(t < 2 * nside, t, 4 * nside - 2 - t)
+    a = (tn + 1.0) ** 2 / (3.0 * nside**2)
+    z = ring_z(nside)
+    return np.where(tn < nside - 1, a * (2.0 - a), (1.0 - z) * (1.0 + z))
+
+
 def ring_theta(nside):
     """theta of every ring, north to south, as the reference derives it (arccos of z)."""
     return np.arccos(ring_z(nside))
@@ -178,13 +189,19 @@ def legendre_by_l(mmax, lmax, x):
         p2, p1 = p1, pl
 
 
-def legendre_column(m, lmax, x):
-    """Pbar_l^m(x) for one m and l < lmax (spot oracle; O(lmax * len(x)) memory)."""
+def legendre_column(m, lmax, x, s2=None):
+    """Pbar_l^m(x) for one m and l < lmax (spot oracle; O(lmax * len(x)) memory).
+
+    The diagonal uses sin^2 = (1 + x)(1 - x) as the reference does, or ``s2``
+    when given."""
     x = np.asarray(x, dtype=np.float64)
     out = np.zeros((lmax, x.size))
     d = np.full(x.shape, 1.0 / np.sqrt(4 * np.pi))
     for l in range(1, m + 1):
-        d = np.sqrt((2 * l + 1) * (1 + x) * (1 - x) / 2 / l) * d
+        if s2 is None:  # the reference's operation order (cuhpx/sht_tools.py:208)
+            d = np.sqrt((2 * l + 1) * (1 + x) * (1 - x) / 2 / l) * d
+        else:
+            d = np.sqrt((2 * l + 1) * s2 / 2 / l) * d
     if m < lmax:
         out[m] = d
     if m + 1 < lmax:
@@ -193,6 +210,34 @@ def legendre_column(m, lmax, x):
         f1, f2 = _rec_coeffs(l, m)
         out[l] = x * f1 * out[l - 1] - f2 * out[l - 2]
     return out
+
+
+def legendre_column_extended(m, lmax, x, s2):
+    """``legendre_column`` carried in 80-bit extended precision (np.longdouble,
+    exponent range to 1e-4951) and returned as float64.
+
+    The reference's FP64 diagonal Pbar_m^m ~ sin^m(theta) goes subnormal below
+    1e-308 for high m near the poles (at nside 1024, orders above ~500); where
+    the recurrence then grows those values back to O(1e-2) within l < L they
+    carry the subnormal's lost bits (relative errors up to ~1e-6 in orders near
+    1023).  Here nothing underflows that matters, so this is the accurate
+    column at the given nodes."""
+    ld = np.longdouble
+    x = np.asarray(x, dtype=np.float64).astype(ld)
+    sq = np.asarray(s2, dtype=np.float64).astype(ld)
+    out = np.zeros((lmax, x.size), dtype=ld)
+    d = np.full(x.shape, ld(1) / np.sqrt(ld(4) * ld(np.pi)), dtype=ld)
+    for l in range(1, m + 1):
+        d = np.sqrt(ld(2 * l + 1) * sq / ld(2 * l)) * d
+    if m < lmax:
+        out[m] = d
+    if m + 1 < lmax:
+        out[m + 1] = np.sqrt(ld(2 * (m + 1) + 1)) * x * d
+    for l in range(m + 2, lmax):
+        f1 = np.sqrt(ld(2 * l - 1) / ld(l - m) * ld(2 * l + 1) / ld(l + m))
+        f2 = np.sqrt(ld(l + m - 1) / ld(l - m) * ld(2 * l + 1) / ld(2 * l - 3) * ld(l - m - 1) / ld(l + m))
+        out[l] = x * f1 * out[l - 1] - f2 * out[l - 2]
+    return out.astype(np.float64)
 
 
 # --------------------------------------------------------------------------- ring FFTs
@@ -287,19 +332,31 @@ def isht(alm, nside, lmax=None, mmax=None, phase_dtype=np.complex128):
     return ring_irfft(ftm, M, nside, phase_dtype)
 
 
-def sht_spot(f, nside, lmax, mmax, ms, quad_weights="ring"):
+def sht_spot(f, nside, lmax, mmax, ms, quad_weights="ring", nodes="reference"):
     """Forward SHT restricted to the columns ``ms`` (returns [..., L, len(ms)]).
 
     Same algorithm as ``sht`` with one Legendre column at a time, so memory is
     O(lmax * rings) and it runs at nside 1024 on a few maps.
+
+    ``nodes="reference"`` follows the reference exactly: Pbar at
+    cos(arccos z_t), sin^2 = (1 + x)(1 - x), FP64 recurrence from the FP64
+    diagonal (cuhpx/hpx_sht.py:192; cuhpx/sht_tools.py:204-214), including the
+    subnormal diagonal of high orders near the poles that costs the
+    reference up to ~1e-6 relative accuracy in orders near M/2 at nside 1024
+    (see ``legendre_column_extended``).  ``nodes="exact"`` evaluates Pbar at
+    the ring's z_t with sin^2 from ``ring_sin2`` by the same recurrence in
+    extended precision: the accurate transform at the nodes the CUDA plan uses.
     """
     L, M = lmax, mmax
     ftm = ring_rfft(f, M, nside)
     w = ring_weights(nside, quad_weights)
-    x = np.cos(ring_theta(nside))
+    if nodes == "exact":
+        x, s2 = ring_z(nside), ring_sin2(nside)
+    else:
+        x, s2 = np.cos(ring_theta(nside)), None
     out = np.zeros(ftm.shape[:-2] + (L, len(ms)), dtype=np.complex128)
     for j, m in enumerate(ms):
-        P = legendre_column(m, L, x)  # [L, R]
+        P = legendre_column(m, L, x) if s2 is None else legendre_column_extended(m, L, x, s2)  # [L, R]
         out[..., :, j] = np.einsum("...t,lt->...l", ftm[..., :, m] * w, P)
     return out
 

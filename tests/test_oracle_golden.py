@@ -146,3 +146,47 @@ def test_cpu_baseline_port_matches_reference_goldens(ref_cpu):
     d = load("cfg1_n32.npz")
     assert rel(ref_cpu.sht(d["f"], 32, 65, 65), d["alm64"]) < 1e-7
     assert rel(ref_cpu.isht(d["alm64"], 32), d["map64"]) < 1e-7
+
+
+def test_spot_oracle_exact_nodes_close_to_reference_nodes():
+    # the exact nodes differ from the reference's cos(arccos z) by roundings only
+    d = load("cfg1_n32.npz")
+    ms = [0, 1, 7, 31, 64]
+    a = O.sht_spot(d["f"], 32, 65, 65, ms)
+    b = O.sht_spot(d["f"], 32, 65, 65, ms, nodes="exact")
+    assert 0 < rel(b, a) < 1e-12
+    s2 = O.ring_sin2(32)
+    z = O.ring_z(32)
+    assert np.abs(s2 - (1 - z) * (1 + z)).max() < 1e-15
+
+
+def test_extended_legendre_against_50_digit_recurrence():
+    # Near the poles the reference's FP64 diagonal Pbar_m^m goes subnormal for
+    # high orders, and the recurrence carries the lost bits up to degrees where
+    # the values matter.  At nside 1024, m = 1023, ring 624 (sin theta = 0.483)
+    # the FP64 diagonal is the smallest subnormal and Pbar_2046^1023 comes out
+    # 0 instead of 3.3e-4; at ring 625 it is 13% off.  The extended-precision
+    # column of the exact-node spot oracle matches the same recurrence run with
+    # 50 digits.
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 50
+    N, L, m = 1024, 2047, 1023
+    rings = np.array([600, 624, 625, 660, 700])
+    z = O.ring_z(N)[rings]
+    s2 = O.ring_sin2(N)[rings]
+    ext = O.legendre_column_extended(m, L, z, s2)
+    ref = O.legendre_column(m, L, z, s2)
+    for k in range(len(rings)):
+        x, sq = mpmath.mpf(z[k]), mpmath.mpf(s2[k])
+        d = 1 / mpmath.sqrt(4 * mpmath.pi)
+        for l in range(1, m + 1):
+            d = mpmath.sqrt((2 * l + 1) * sq / (2 * l)) * d
+        p2, p1 = d, mpmath.sqrt(2 * m + 3) * x * d
+        for l in range(m + 2, L):
+            f1 = mpmath.sqrt(mpmath.mpf(2 * l - 1) / (l - m) * (2 * l + 1) / (l + m))
+            f2 = mpmath.sqrt(mpmath.mpf(l + m - 1) / (l - m) * (2 * l + 1) / (2 * l - 3) * (l - m - 1) / (l + m))
+            p2, p1 = p1, x * f1 * p1 - f2 * p2
+        want = float(p1)  # degree L - 1
+        assert abs(ext[L - 1, k] - want) <= 1e-14 * abs(want), rings[k]
+    assert ref[L - 1, 1] == 0.0 and abs(ext[L - 1, 1] - 3.26e-4) < 1e-6
+    assert abs(ref[L - 1, 2] / ext[L - 1, 2] - 1) > 0.1
