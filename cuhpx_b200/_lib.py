@@ -131,6 +131,17 @@ def load():
         return lib
 
 
+def load_path(path):
+    """A separate copy of the library from `path` (a checker build), with the
+    same signatures; it shares no state with the one load() returns."""
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
 def check(status, plan=None):
     if status != HPX_OK:
         lib = load()

@@ -79,6 +79,26 @@ def build(force=False, debug=False, verbose=False, defines=(), out=None):
     return target
 
 
+# Checker builds of the same sources (test infrastructure, never loaded by the
+# package): name -> (defines, file).
+#   waittest  every bounded pipeline wait gives up after 1 ms and the tensor-core
+#             kernels withhold their TMA loads, so their waits run out: the
+#             failure-detection test checks that a call then ends with
+#             HPX_ERR_TIMEOUT and leaves the device usable
+VARIANTS = {
+    "waittest": (["HPX_WAIT_LIMIT_NS=1000000ull", "HPX_TEST_WITHHOLD_TMA_LOADS=1"],
+                 os.path.join(HERE, "libhpx_b200_waittest.so")),
+}
+
+
+def build_variant(name, force=False):
+    """Compile one checker build (see VARIANTS) if it is older than the sources."""
+    defines, path = VARIANTS[name]
+    if not force and os.path.exists(path) and all(os.path.getmtime(f) <= os.path.getmtime(path) for f in _deps()):
+        return path
+    return build(defines=defines, out=path)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")

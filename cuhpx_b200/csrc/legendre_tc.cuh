@@ -95,6 +95,16 @@ __host__ __device__ constexpr int fwd_tile_c0(int y) { return y >> 8; }
 __host__ __device__ constexpr int inv_tile_rb(int y) { return y & 0xffff; }
 __host__ __device__ constexpr int inv_tile_c0(int y) { return y >> 16; }
 
+// Failure-detection test builds only (-DHPX_TEST_WITHHOLD_TMA_LOADS): the TMA
+// thread announces each stage's bytes but issues no load, so the MMA thread's
+// bounded wait for the stage runs out, the kernel drains and returns, and
+// hpx_plan_check reports HPX_ERR_TIMEOUT.  The product library never has it.
+#ifdef HPX_TEST_WITHHOLD_TMA_LOADS
+constexpr bool kWithholdTmaLoads = true;
+#else
+constexpr bool kWithholdTmaLoads = false;
+#endif
+
 // analysis: 6 stages of 16 rings (32 KB: A 4 x 4 KB, B 4 x 4 KB)
 constexpr int kFStages = 6;
 constexpr int kFRing = 16;
@@ -495,6 +505,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!tc::mbar_wait(&sh->empty[s], ((it / NS) & 1) ^ 1, err, 11)) goto tma_done;
                     unsigned char* st = stages + s * SB + SB / 2;
                     tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? SB : SB / 2);
+                    if (kWithholdTmaLoads) continue;
                     const int y = t0 + c * RS;  // rings past NP read as zeros (TMA out-of-bounds fill)
                     if (TAB) {
                         // A operand: Pbar for 128 degrees of each parity x RS rings, hi and lo
@@ -804,6 +815,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (!tc::mbar_wait(&sh->empty[s], ((it / kIStages) & 1) ^ 1, err, 21)) goto tma_done;
                     unsigned char* st = stages + s * kIStageBytes + 32768;
                     tc::mbar_arrive_tx(&sh->full_tma[s], TAB ? 65536 : 32768);
+                    if (kWithholdTmaLoads) continue;
                     if (TAB) {
                         // A operand: Pbar^T for 128 rings x 32 degrees of each parity, hi and lo
 #pragma unroll

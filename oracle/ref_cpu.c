@@ -186,3 +186,127 @@ int hpx_ref_isht_contract(const double* alm, const double* x, int R, int L, int 
     free(dg);
     return fail;
 }
+
+/*
+ * The same analysis contraction with the Legendre recurrence carried in
+ * 80-bit extended precision (long double, exponent range to 1e-4951) at the
+ * nodes x_t with sin^2(theta_t) = s2_t given by the caller: the reference's
+ * FP64 diagonal Pbar_m^m ~ sin^m(theta) goes subnormal for high orders near
+ * the poles, and the recurrence carries the lost bits up to degrees where the
+ * values matter.  This is the accurate transform the CUDA FP64 path is checked
+ * against at large nside.  Products with the spectra are summed in long double.
+ */
+int hpx_ref_sht_contract_ext(const double* ftm, const double* w, const double* x, const double* s2, int R, int L,
+                             int M, double* alm) {
+    memset(alm, 0, sizeof(double) * 2 * (size_t)L * M);
+    int fail = 0;
+#pragma omp parallel
+    {
+        long double* buf = (long double*)malloc(sizeof(long double) * 5 * (size_t)R);
+        if (!buf) {
+#pragma omp atomic write
+            fail = 1;
+        }
+#pragma omp for schedule(dynamic, 1)
+        for (int m = 0; m < M; ++m) {
+            if (!buf || m >= L) continue;
+            long double *fr = buf, *fi = buf + R, *p2 = buf + 2 * R, *p1 = buf + 3 * R, *xl = buf + 4 * R;
+            for (int t = 0; t < R; ++t) {
+                fr[t] = (long double)w[t] * ftm[2 * ((size_t)t * M + m)];
+                fi[t] = (long double)w[t] * ftm[2 * ((size_t)t * M + m) + 1];
+                xl[t] = x[t];
+                long double d = 1.0L / sqrtl(4.0L * 3.14159265358979323846264338327950288L);
+                for (int l = 1; l <= m; ++l) d = sqrtl((2.0L * l + 1.0L) * (long double)s2[t] / (2.0L * l)) * d;
+                p2[t] = d;
+                p1[t] = sqrtl(2.0L * (m + 1) + 1.0L) * xl[t] * d;
+            }
+            long double ar = 0, ai = 0, br = 0, bi = 0;
+            for (int t = 0; t < R; ++t) {
+                ar += p2[t] * fr[t];
+                ai += p2[t] * fi[t];
+                br += p1[t] * fr[t];
+                bi += p1[t] * fi[t];
+            }
+            alm[2 * ((size_t)m * M + m)] = (double)ar;
+            alm[2 * ((size_t)m * M + m) + 1] = (double)ai;
+            if (m + 1 < L) {
+                alm[2 * ((size_t)(m + 1) * M + m)] = (double)br;
+                alm[2 * ((size_t)(m + 1) * M + m) + 1] = (double)bi;
+            }
+            for (int l = m + 2; l < L; ++l) {
+                const long double f1 = sqrtl((2.0L * l - 1.0L) / (l - m) * (2.0L * l + 1.0L) / (l + m));
+                const long double f2 = sqrtl((l + m - 1.0L) / (l - m) * (2.0L * l + 1.0L) / (2.0L * l - 3.0L) *
+                                             (l - m - 1.0L) / (l + m));
+                long double sr = 0, si = 0;
+                for (int t = 0; t < R; ++t) {
+                    const long double v = xl[t] * f1 * p1[t] - f2 * p2[t];
+                    p2[t] = p1[t];
+                    p1[t] = v;
+                    sr += v * fr[t];
+                    si += v * fi[t];
+                }
+                alm[2 * ((size_t)l * M + m)] = (double)sr;
+                alm[2 * ((size_t)l * M + m) + 1] = (double)si;
+            }
+        }
+        free(buf);
+    }
+    return fail;
+}
+
+/* The synthesis contraction in extended precision (as hpx_ref_sht_contract_ext). */
+int hpx_ref_isht_contract_ext(const double* alm, const double* x, const double* s2, int R, int L, int M,
+                              double* ftm) {
+    int fail = 0;
+#pragma omp parallel
+    {
+        long double* buf = (long double*)malloc(sizeof(long double) * 5 * (size_t)R);
+        if (!buf) {
+#pragma omp atomic write
+            fail = 1;
+        }
+#pragma omp for schedule(dynamic, 1)
+        for (int m = 0; m < M; ++m) {
+            if (!buf) continue;
+            long double *gr = buf, *gi = buf + R, *p2 = buf + 2 * R, *p1 = buf + 3 * R, *xl = buf + 4 * R;
+            if (m >= L) {
+                for (int t = 0; t < R; ++t) {
+                    ftm[2 * ((size_t)t * M + m)] = 0.0;
+                    ftm[2 * ((size_t)t * M + m) + 1] = 0.0;
+                }
+                continue;
+            }
+            const long double a0r = alm[2 * ((size_t)m * M + m)], a0i = alm[2 * ((size_t)m * M + m) + 1];
+            const long double a1r = m + 1 < L ? alm[2 * ((size_t)(m + 1) * M + m)] : 0.0;
+            const long double a1i = m + 1 < L ? alm[2 * ((size_t)(m + 1) * M + m) + 1] : 0.0;
+            for (int t = 0; t < R; ++t) {
+                xl[t] = x[t];
+                long double d = 1.0L / sqrtl(4.0L * 3.14159265358979323846264338327950288L);
+                for (int l = 1; l <= m; ++l) d = sqrtl((2.0L * l + 1.0L) * (long double)s2[t] / (2.0L * l)) * d;
+                p2[t] = d;
+                p1[t] = sqrtl(2.0L * (m + 1) + 1.0L) * xl[t] * d;
+                gr[t] = p2[t] * a0r + (m + 1 < L ? p1[t] * a1r : 0.0L);
+                gi[t] = p2[t] * a0i + (m + 1 < L ? p1[t] * a1i : 0.0L);
+            }
+            for (int l = m + 2; l < L; ++l) {
+                const long double f1 = sqrtl((2.0L * l - 1.0L) / (l - m) * (2.0L * l + 1.0L) / (l + m));
+                const long double f2 = sqrtl((l + m - 1.0L) / (l - m) * (2.0L * l + 1.0L) / (2.0L * l - 3.0L) *
+                                             (l - m - 1.0L) / (l + m));
+                const long double ar = alm[2 * ((size_t)l * M + m)], ai = alm[2 * ((size_t)l * M + m) + 1];
+                for (int t = 0; t < R; ++t) {
+                    const long double v = xl[t] * f1 * p1[t] - f2 * p2[t];
+                    p2[t] = p1[t];
+                    p1[t] = v;
+                    gr[t] += v * ar;
+                    gi[t] += v * ai;
+                }
+            }
+            for (int t = 0; t < R; ++t) {
+                ftm[2 * ((size_t)t * M + m)] = (double)gr[t];
+                ftm[2 * ((size_t)t * M + m) + 1] = (double)gi[t];
+            }
+        }
+        free(buf);
+    }
+    return fail;
+}

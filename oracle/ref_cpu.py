@@ -6,7 +6,12 @@ cuHPX's CPU transforms (cuhpx/hpx_sht.py:173-283) run, per call, one
 spectra with the precomputed Legendre table.  This module does the same with
 the contraction in C (``ref_cpu.c``, OpenMP over the orders), regenerating
 the table's values per order by the reference's recurrence instead of holding
-it (68.6 GB at nside 1024, L = M = 2047).  It is what ``bench.py`` times as
+it (68.6 GB at nside 1024, L = M = 2047).  ``sht_extended``/``isht_extended``
+run the same recurrence in 80-bit extended precision at the rings' exact
+nodes: at nside 1024 the reference's FP64 diagonal goes subnormal for high
+orders near the poles and its recurrence then diverges (values up to ~40
+where the true ones are ~1e-35), so large-nside parity is checked against
+those.  It is what ``bench.py`` times as
 the reference's CPU implementation; ``tests/test_oracle_golden.py`` checks it
 against the golden-pinned oracle.  The product never imports it.
 
@@ -47,6 +52,8 @@ def load():
         dp = ctypes.POINTER(ctypes.c_double)
         lib.hpx_ref_sht_contract.argtypes = [dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         lib.hpx_ref_isht_contract.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        lib.hpx_ref_sht_contract_ext.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        lib.hpx_ref_isht_contract_ext.argtypes = [dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         lib.hpx_ref_threads.restype = ctypes.c_int
         lib.hpx_ref_set_threads.argtypes = [ctypes.c_int]
         _lib = lib
@@ -78,6 +85,23 @@ def sht(f, nside, lmax, mmax, quad_weights="ring"):
     return alm
 
 
+def sht_extended(f, nside, lmax, mmax, quad_weights="ring"):
+    """Forward SHT of one map with the Legendre recurrence in 80-bit extended
+    precision at the rings' z_t (sin^2 from ``hpx_oracle.ring_sin2``): the
+    accurate analysis at large nside, where the reference's FP64 diagonal
+    underflows for high orders near the poles."""
+    lib = load()
+    ftm = np.ascontiguousarray(O.ring_rfft(np.asarray(f, dtype=np.float64), mmax, nside))
+    w = np.ascontiguousarray(O.ring_weights(nside, quad_weights))
+    x = np.ascontiguousarray(O.ring_z(nside))
+    s2 = np.ascontiguousarray(O.ring_sin2(nside))
+    alm = np.empty((lmax, mmax), dtype=np.complex128)
+    if lib.hpx_ref_sht_contract_ext(_ptr(ftm.view(np.float64)), _ptr(w), _ptr(x), _ptr(s2), x.size, lmax, mmax,
+                                    _ptr(alm.view(np.float64))):
+        raise MemoryError("ref_cpu: allocation failed")
+    return alm
+
+
 def isht(alm, nside):
     """Inverse SHT of one coefficient set: [L, M] complex -> [npix] (cuhpx/hpx_sht.py:268-283)."""
     lib = load()
@@ -86,6 +110,21 @@ def isht(alm, nside):
     x = np.ascontiguousarray(np.cos(O.ring_theta(nside)))
     ftm = np.empty((x.size, M), dtype=np.complex128)
     if lib.hpx_ref_isht_contract(_ptr(alm.view(np.float64)), _ptr(x), x.size, L, M, _ptr(ftm.view(np.float64))):
+        raise MemoryError("ref_cpu: allocation failed")
+    return O.ring_irfft(ftm, M, nside)
+
+
+def isht_extended(alm, nside):
+    """Inverse SHT of one coefficient set with the Legendre recurrence in 80-bit
+    extended precision at the rings' z_t (see ``sht_extended``)."""
+    lib = load()
+    alm = np.ascontiguousarray(alm, dtype=np.complex128)
+    L, M = alm.shape
+    x = np.ascontiguousarray(O.ring_z(nside))
+    s2 = np.ascontiguousarray(O.ring_sin2(nside))
+    ftm = np.empty((x.size, M), dtype=np.complex128)
+    if lib.hpx_ref_isht_contract_ext(_ptr(alm.view(np.float64)), _ptr(x), _ptr(s2), x.size, L, M,
+                                     _ptr(ftm.view(np.float64))):
         raise MemoryError("ref_cpu: allocation failed")
     return O.ring_irfft(ftm, M, nside)
 

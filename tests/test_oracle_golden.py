@@ -190,3 +190,27 @@ def test_extended_legendre_against_50_digit_recurrence():
         assert abs(ext[L - 1, k] - want) <= 1e-14 * abs(want), rings[k]
     assert ref[L - 1, 1] == 0.0 and abs(ext[L - 1, 1] - 3.26e-4) < 1e-6
     assert abs(ref[L - 1, 2] / ext[L - 1, 2] - 1) > 0.1
+
+
+def test_reference_fp64_recurrence_diverges_at_nside1024():
+    # The reference's own table at nside 1024, L = 2047: for m = 1198 on the
+    # south ring 3445 (sin theta = 0.5006) its FP64 diagonal is subnormal, the
+    # start pair is inconsistent and the three-term recurrence picks up the
+    # wrong solution: Pbar_2046^1198 comes out ~40 where the true value is
+    # ~1e-35.  The extended-precision column does not.
+    N, L, m, t = 1024, 2047, 1198, 3445
+    z, s2 = O.ring_z(N)[[t]], O.ring_sin2(N)[[t]]
+    ref = O.legendre_column(m, L, np.cos(O.ring_theta(N))[[t]])
+    ext = O.legendre_column_extended(m, L, z, s2)
+    assert abs(ref[L - 1, 0]) > 1.0
+    assert abs(ext[L - 1, 0]) < 1e-30
+
+
+@pytest.mark.parametrize("nside,L,M", [(8, 17, 17), (16, 33, 33), (32, 65, 65)])
+def test_cpu_port_extended_matches_oracle(ref_cpu, nside, L, M):
+    # where nothing underflows, the extended-precision port agrees with the oracle
+    rng = np.random.default_rng(nside)
+    f = rng.standard_normal(12 * nside * nside)
+    a = O.sht(f, nside, L, M)
+    assert rel(ref_cpu.sht_extended(f, nside, L, M), a) < 1e-12
+    assert rel(ref_cpu.isht_extended(a, nside), O.isht(a, nside)) < 1e-12
