@@ -3,11 +3,13 @@
 Drop-in for the SHT path of cuHPX: ``SHTCUDA``, ``iSHTCUDA``, ``Grid`` and
 ``Regridding``, and for its pixel-order remapping (``ring2nest``,
 ``nest2ring``, ``nest2flat``, ``flat2nest``, ``ring2flat``, ``flat2ring``,
-``flat2flat``).  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
+``flat2flat``), with the healpy a_lm packing beside them (``alm_to_healpy``,
+``healpy_to_alm``).  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
 C ABI in ``include/hpx_b200.h``); there is no CPU fallback.
 """
 
 from . import sht_tools
+from .healpy_alm import alm_to_healpy, healpy_index, healpy_size, healpy_to_alm
 from .hpx_sht import (LatLonPlan, Plan, SHTCUDA, SHTFunction, clear_plan_cache, get_latlon_plan, get_plan, iSHTCUDA,
                       iSHTFunction)
 from .latlon import InverseRealSHT, RealSHT
@@ -40,4 +42,8 @@ __all__ = [
     "ring2flat",
     "flat2ring",
     "flat2flat",
+    "alm_to_healpy",
+    "healpy_to_alm",
+    "healpy_size",
+    "healpy_index",
 ]

@@ -92,6 +92,10 @@ SIGNATURES = {
                             ctypes.POINTER(_i64), _vp, _sz, _vp], ctypes.c_int),
     "hpx_remap": ([_vp, _vp, _i64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                    ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp], ctypes.c_int),
+    "hpx_alm_to_healpy": ([_vp, _vp, _i64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp],
+                          ctypes.c_int),
+    "hpx_healpy_to_alm": ([_vp, _vp, _i64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp],
+                          ctypes.c_int),
     "hpx_plan_info": (
         [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
         ctypes.c_int,

@@ -36,6 +36,7 @@
 #include "hpx_kernels.cuh"
 #include "legendre_tc.cuh"
 #include "hpx_remap.cuh"
+#include "hpx_healpy.cuh"
 
 using namespace hpx;
 
@@ -1369,6 +1370,48 @@ int remap_side(int32_t order, int32_t origin, int32_t clockwise, RemapSide* sd, 
 
 }  // namespace
 
+namespace {
+template <typename E>
+int launch_healpy(const void* in, void* out, int64_t batch, int L, int M, int cs, bool pack, cudaStream_t st) {
+    const int Mk = std::min(M, L);
+    const dim3 grid((unsigned)(((pack ? Mk : M) + kHpTile - 1) / kHpTile), (unsigned)((L + kHpTile - 1) / kHpTile), 1);
+    const int64_t src_stride = pack ? (int64_t)L * M : healpy_size(L, M);
+    const int64_t dst_stride = pack ? healpy_size(L, M) : (int64_t)L * M;
+    for (int64_t b = 0; b < batch; b += 65535) {
+        dim3 g = grid;
+        g.z = (unsigned)std::min<int64_t>(65535, batch - b);
+        const E* s = (const E*)in + b * src_stride;
+        E* d = (E*)out + b * dst_stride;
+        if (pack) k_healpy<E, true><<<g, dim3(kHpTile, 8), 0, st>>>(s, d, L, M, cs);
+        else k_healpy<E, false><<<g, dim3(kHpTile, 8), 0, st>>>(s, d, L, M, cs);
+        HPX_CUDA_TRY(cudaGetLastError());
+    }
+    return HPX_OK;
+}
+
+int healpy_call(const void* in, void* out, int64_t batch, int32_t lmax, int32_t mmax, int32_t elem_bytes,
+                int32_t cs_phase, bool pack, void* stream) {
+    if (batch < 0) return set_err(HPX_ERR_INVALID_ARG, "negative batch");
+    if (lmax < 1 || mmax < 1 || lmax > 65536 || mmax > 65536)
+        return set_err(HPX_ERR_INVALID_ARG, "lmax and mmax must be in [1, 65536]");
+    if (elem_bytes != 8 && elem_bytes != 16)
+        return set_err(HPX_ERR_INVALID_ARG, "elem_bytes must be 8 (complex float) or 16 (complex double)");
+    if (batch == 0) return HPX_OK;
+    if (!in || !out) return set_err(HPX_ERR_INVALID_ARG, "null pointer");
+    if ((((uintptr_t)in) | ((uintptr_t)out)) % (uintptr_t)elem_bytes)
+        return set_err(HPX_ERR_INVALID_ARG, "in and out must be aligned to elem_bytes");
+    const uint64_t per = (uint64_t)std::max<int64_t>((int64_t)lmax * mmax, healpy_size(lmax, mmax)) * elem_bytes;
+    if ((uint64_t)batch > (1ull << 62) / per) return set_err(HPX_ERR_INVALID_ARG, "batch too large");
+    const uint64_t in_bytes = (uint64_t)batch * elem_bytes * (pack ? (uint64_t)lmax * mmax : (uint64_t)healpy_size(lmax, mmax));
+    const uint64_t out_bytes = (uint64_t)batch * elem_bytes * (pack ? (uint64_t)healpy_size(lmax, mmax) : (uint64_t)lmax * mmax);
+    const uintptr_t a = (uintptr_t)in, b = (uintptr_t)out;
+    if (a < b + out_bytes && b < a + in_bytes) return set_err(HPX_ERR_INVALID_ARG, "in and out overlap");
+    cudaStream_t st = (cudaStream_t)stream;
+    return elem_bytes == 8 ? launch_healpy<float2>(in, out, batch, lmax, mmax, cs_phase != 0, pack, st)
+                           : launch_healpy<double2>(in, out, batch, lmax, mmax, cs_phase != 0, pack, st);
+}
+}  // namespace
+
 extern "C" {
 
 int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, int32_t elem_bytes, int32_t src_order,
@@ -1407,6 +1450,16 @@ int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, int32_t e
         case 8: return launch_remap<unsigned long long>(in, out, batch, nside, src, dst, st);
         default: return launch_remap<uint4>(in, out, batch, nside, src, dst, st);
     }
+}
+
+int hpx_alm_to_healpy(const void* alm, void* packed, int64_t batch, int32_t lmax, int32_t mmax, int32_t elem_bytes,
+                      int32_t cs_phase, void* stream) {
+    return healpy_call(alm, packed, batch, lmax, mmax, elem_bytes, cs_phase, true, stream);
+}
+
+int hpx_healpy_to_alm(const void* packed, void* alm, int64_t batch, int32_t lmax, int32_t mmax, int32_t elem_bytes,
+                      int32_t cs_phase, void* stream) {
+    return healpy_call(packed, alm, batch, lmax, mmax, elem_bytes, cs_phase, false, stream);
 }
 
 int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream) {

@@ -228,6 +228,24 @@ HPX_API int hpx_remap(const void* in, void* out, int64_t batch, int32_t nside, i
                       int32_t src_order, int32_t src_origin, int32_t src_clockwise, int32_t dst_order,
                       int32_t dst_origin, int32_t dst_clockwise, void* stream);
 
+/* healpy a_lm packing.  This library's coefficients are dense
+ * [batch][lmax][mmax] complex (zeros for m > l); healpy keeps the m <= l
+ * triangle in one vector per map, order by order:
+ *   packed[m (2 lmax - 1 - m) / 2 + l] = alm[l][m],  m <= l < lmax, m < min(mmax, lmax)
+ * (healpy's own lmax is this lmax - 1), packed length
+ * min(mmax,lmax) * lmax - min(mmax,lmax) (min(mmax,lmax) - 1) / 2.
+ * cs_phase != 0 multiplies order m by (-1)^m, the Condon-Shortley factor
+ * between this library's (cuHPX's) phase convention and healpy's.
+ * elem_bytes: 8 (complex float) or 16 (complex double).  Unpacking writes the
+ * whole dense array, zeros included.  Runs on `stream`; allocates nothing.
+ * Replaces the index map cuHPX states in
+ * tests/reproduce_difference_between_healpy_cuhpx.py:58-81 (hp_getidx,
+ * flm_hp_to_2d). */
+HPX_API int hpx_alm_to_healpy(const void* alm, void* packed, int64_t batch, int32_t lmax, int32_t mmax,
+                              int32_t elem_bytes, int32_t cs_phase, void* stream);
+HPX_API int hpx_healpy_to_alm(const void* packed, void* alm, int64_t batch, int32_t lmax, int32_t mmax,
+                              int32_t elem_bytes, int32_t cs_phase, void* stream);
+
 /* Plan geometry queries. */
 HPX_API int hpx_plan_info(hpx_plan_t plan, int32_t* nside, int32_t* lmax, int32_t* mmax, int32_t* precision);
 

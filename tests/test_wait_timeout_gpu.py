@@ -89,9 +89,10 @@ def test_tensor_core_wait_runs_out_with_a_status(waitlib, cuda, precision, flags
 def test_device_usable_after_timeouts(waitlib, cuda):
     rng = np.random.default_rng(5)
     f = rng.standard_normal((2, NPIX))
-    ref = O.sht(f, NSIDE, L, L)
     stream = torch.cuda.current_stream(cuda).cuda_stream
     # the checker library's SIMT path has no pipeline waits and computes normally
+    # (its plans here carry no ring weights: uniform quadrature)
+    ref = O.sht(f, NSIDE, L, L, quad_weights="none")
     plan = make_plan(waitlib, FP32)
     try:
         x = torch.from_numpy(f).float().to(cuda)
@@ -104,6 +105,8 @@ def test_device_usable_after_timeouts(waitlib, cuda):
         waitlib.hpx_plan_destroy(plan)
     # and the product library's tensor-core path on the same device
     import cuhpx_b200 as hpx
+
+    ref = O.sht(f, NSIDE, L, L)
 
     got = hpx.SHTCUDA(NSIDE, lmax=L, mmax=L, precision="f16x3")(torch.from_numpy(f).float().to(cuda))
     err = np.linalg.norm(got.cpu().numpy() - ref) / np.linalg.norm(ref)
