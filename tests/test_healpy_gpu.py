@@ -49,15 +49,17 @@ def test_round_trip_with_the_transform(cuda):
     # healpy-packed coefficients -> dense -> iSHT -> SHT -> packed
     import cuhpx_b200 as hpx
 
-    nside, L = 16, 33
+    # band limit within what nside 16 resolves; two Jacobi iterations remove
+    # the quadrature error
+    nside, L = 16, 17
     rng = np.random.default_rng(1)
     a = rng.standard_normal((2, L, L)) + 1j * rng.standard_normal((2, L, L))
     a = np.where(np.arange(L)[None, None, :] <= np.arange(L)[None, :, None], a, 0)
     a[..., 0] = a[..., 0].real
     p = hpx.alm_to_healpy(torch.from_numpy(a).to(cuda), csphase=True)
     f = hpx.iSHTCUDA(nside, lmax=L, mmax=L)(hpx.healpy_to_alm(p, L, L, csphase=True))
-    back = hpx.alm_to_healpy(hpx.SHTCUDA(nside, lmax=L, mmax=L, refine_iters=0)(f), csphase=True)
-    assert torch.allclose(back, p, atol=1e-3)
+    back = hpx.alm_to_healpy(hpx.SHTCUDA(nside, lmax=L, mmax=L, refine_iters=2)(f), csphase=True)
+    assert float((back - p).abs().norm() / p.abs().norm()) < 1e-6
 
 
 def test_argument_errors(cuda):
