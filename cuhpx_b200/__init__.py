@@ -1,7 +1,7 @@
 """hpx_b200: HEALPix spherical-harmonic transforms for NVIDIA B200 (sm_100a).
 
-Drop-in for the SHT path of cuHPX: ``SHTCUDA``, ``iSHTCUDA``, ``Grid`` and
-``Regridding``, and for its pixel-order remapping (``ring2nest``,
+Drop-in for the SHT path of cuHPX: ``SHTCUDA``, ``iSHTCUDA``, the spin-1
+``VectorSHTCUDA`` / ``VectoriSHTCUDA``, ``Grid`` and ``Regridding``, and for its pixel-order remapping (``ring2nest``,
 ``nest2ring``, ``nest2flat``, ``flat2nest``, ``ring2flat``, ``flat2ring``,
 ``flat2flat``), with the healpy a_lm packing beside them (``alm_to_healpy``,
 ``healpy_to_alm``).  The transforms run in ``libhpx_b200.so`` (hand-written CUDA,
@@ -16,10 +16,13 @@ from .latlon import InverseRealSHT, RealSHT
 from .ragged import RaggedISHT, RaggedSHT, split_by_offsets
 from .regrid import Grid, Regridding
 from .remap import flat2flat, flat2nest, flat2ring, nest2flat, nest2ring, ring2flat, ring2nest
+from .vector import VectoriSHTCUDA, VectorSHTCUDA
 
 __all__ = [
     "SHTCUDA",
     "iSHTCUDA",
+    "VectorSHTCUDA",
+    "VectoriSHTCUDA",
     "SHTFunction",
     "iSHTFunction",
     "Plan",

@@ -81,6 +81,10 @@ SIGNATURES = {
     "hpx_sht_inverse_adjoint": ([_vp, _vp, _vp, _i64, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_refined": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_sht_forward_noalloc": ([_vp, _vp, _vp, _i64, _vp], ctypes.c_int),
+    "hpx_vsht_forward": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
+    "hpx_vsht_inverse": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
+    "hpx_vsht_forward_adjoint": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
+    "hpx_vsht_inverse_adjoint": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_plan_table_bytes": ([_vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hpx_plan_table_stream_bytes": ([_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz)], ctypes.c_int),
     "hpx_plan_create_latlon": ([ctypes.POINTER(HpxLatLonDesc), ctypes.POINTER(_vp)], ctypes.c_int),

@@ -37,6 +37,7 @@
 #include "legendre_tc.cuh"
 #include "hpx_remap.cuh"
 #include "hpx_healpy.cuh"
+#include "vector.cuh"
 
 using namespace hpx;
 
@@ -279,6 +280,8 @@ int create_typed(hpx_plan_s* P) {
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_vleg_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_vleg_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_inv_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     return HPX_OK;
 }
@@ -1088,6 +1091,70 @@ struct Pipeline {
 
 enum Op { kForward, kInverse, kForwardAdjoint, kInverseAdjoint, kForwardRefined };
 
+// Spin-1 transforms of a plan built with L+1 degrees and M+1 orders (see
+// vector.cuh): maps [batch][2][npix] <-> coefficients [batch][2][L][M].  Each
+// pass takes batch_chunk / 2 vector maps, whose 2 components run through the
+// ring stages as batch_chunk scalar maps.
+template <typename T>
+int run_vec(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void* ws, cudaStream_t st, int csphase) {
+    Pipeline<T> pl(P, ws, st);
+    const int Lv = P->L - 1, Mv = P->M - 1;
+    const int C = P->cols();
+    const int64_t vc = std::max(1, P->batch_chunk / 2);
+    const size_t alm_stride = (size_t)2 * Lv * Mv * 2;
+    const size_t map_stride = (size_t)2 * P->npix;
+    for (int64_t b0 = 0; b0 < batch; b0 += vc) {
+        const int nb = (int)std::min<int64_t>(vc, batch - b0);
+        const bool analysis = op == kForward || op == kInverseAdjoint;
+        if (analysis) {
+            const T* map = (const T*)in + b0 * map_stride;
+            T* alm = (T*)out + b0 * alm_stride;
+            pl.ring_fwd(map, 2 * nb, op == kForward ? 0 : 1);
+            typename Pipeline<T>::Timer tm(P, st, kStLegFwd);
+            const int nj = (Lv + VFwdCfg<T>::LT - 1) / VFwdCfg<T>::LT;
+            const dim3 grid((unsigned)(Mv * nj), (unsigned)((C + VFwdCfg<T>::CT - 1) / VFwdCfg<T>::CT));
+            k_vleg_fwd<T><<<grid, 256, vfwd_smem_bytes<T>(), st>>>(
+                pl.spec, C, nb, alm, Lv, Mv, P->L, P->M, P->Lpad, P->geo, P->d_pairs, P->d_lstart, P->d_pstart,
+                P->d_coef, P->d_seeds, csphase, op == kForward ? 1 : 0);
+        } else {
+            const T* alm = (const T*)in + b0 * alm_stride;
+            T* map = (T*)out + b0 * map_stride;
+            {
+                typename Pipeline<T>::Timer tm(P, st, kStLegInv);
+                const int nr = (P->NP + VInvCfg<T>::RBI - 1) / VInvCfg<T>::RBI;
+                const dim3 grid((unsigned)(P->M * nr), (unsigned)((C + VInvCfg<T>::CT - 1) / VInvCfg<T>::CT));
+                k_vleg_inv<T><<<grid, 256, vinv_smem_bytes<T>(), st>>>(alm, nb, pl.spec, C, Lv, Mv, P->L, P->M,
+                                                                       P->Lpad, P->geo, P->d_pairs, P->d_lstart,
+                                                                       P->d_pstart, P->d_coef, csphase,
+                                                                       op == kForwardAdjoint ? 1 : 0);
+            }
+            pl.ring_inv(map, 2 * nb, op == kInverse ? 0 : 1, nullptr);
+        }
+        if (pl.rc != HPX_OK) return pl.rc;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(HPX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    return HPX_OK;
+}
+
+int dispatch_vec(hpx_plan_t plan, Op op, const void* in, void* out, int64_t batch, int32_t csphase, void* ws,
+                 size_t ws_bytes, void* stream) {
+    int rc = check_call(plan, in, out, batch, ws, ws_bytes);
+    if (rc != HPX_OK || batch == 0) return rc;
+    if (plan->nside <= 0) return set_err(HPX_ERR_UNSUPPORTED, "spin-1 transforms are built for HEALPix plans");
+    if (plan->mixed()) return set_err(HPX_ERR_UNSUPPORTED, "spin-1 transforms run on FP32 or FP64 plans");
+    if (plan->L < 2 || plan->M < 2)
+        return set_err(HPX_ERR_INVALID_ARG, "a spin-1 plan needs lmax >= 2 and mmax >= 2 (L+1 and M+1 of the transform)");
+    DeviceGuard g(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    try {
+        return plan->f64 ? run_vec<double>(plan, op, in, out, batch, ws, st, csphase ? 1 : 0)
+                         : run_vec<float>(plan, op, in, out, batch, ws, st, csphase ? 1 : 0);
+    } catch (const std::exception& ex) {
+        return set_err(HPX_ERR_CUDA, ex.what());
+    }
+}
+
 template <typename T>
 int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void* ws, cudaStream_t st, int iters) {
     Pipeline<T> pl(P, ws, st);
@@ -1658,6 +1725,23 @@ int hpx_sht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_gra
 int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, void* ws,
                             size_t ws_bytes, void* stream) {
     return dispatch(plan, kInverseAdjoint, map_grad, alm_grad, batch, ws, ws_bytes, stream);
+}
+
+int hpx_vsht_forward(hpx_plan_t plan, const void* map, void* alm, int64_t batch, int32_t csphase, void* ws,
+                     size_t ws_bytes, void* stream) {
+    return dispatch_vec(plan, kForward, map, alm, batch, csphase, ws, ws_bytes, stream);
+}
+int hpx_vsht_inverse(hpx_plan_t plan, const void* alm, void* map, int64_t batch, int32_t csphase, void* ws,
+                     size_t ws_bytes, void* stream) {
+    return dispatch_vec(plan, kInverse, alm, map, batch, csphase, ws, ws_bytes, stream);
+}
+int hpx_vsht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_grad, int64_t batch, int32_t csphase,
+                             void* ws, size_t ws_bytes, void* stream) {
+    return dispatch_vec(plan, kForwardAdjoint, alm_grad, map_grad, batch, csphase, ws, ws_bytes, stream);
+}
+int hpx_vsht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, int32_t csphase,
+                             void* ws, size_t ws_bytes, void* stream) {
+    return dispatch_vec(plan, kInverseAdjoint, map_grad, alm_grad, batch, csphase, ws, ws_bytes, stream);
 }
 
 int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes) {

@@ -138,6 +138,25 @@ HPX_API int hpx_sht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void*
  * looks it up again (make that call outside stream capture too). */
 HPX_API int hpx_sht_forward_noalloc(hpx_plan_t plan, const void* map, void* alm, int64_t batch, void* stream);
 
+/* Spin-1 (vector) transforms: cuHPX's VectorSHT / VectoriSHT
+ * (cuhpx/hpx_sht.py:286-444, table _precompute_dlegpoly, cuhpx/sht_tools.py:267-304).
+ * A vector map is [batch][2][12*nside^2] (two real components), its
+ * coefficients [batch][2][L][M] complex (spheroidal, toroidal; zeros for
+ * m > l and for l = 0 ... as the reference gives them).  The plan must be a
+ * HEALPix FP32 or FP64 plan created with lmax = L + 1 and mmax = M + 1 (the
+ * table reaches degree L and order M); workspace as hpx_workspace_size.
+ * csphase != 0 negates the odd orders, as the reference's default
+ * csphase=True does.  The adjoints are exact (the reference differentiates
+ * its einsums by autograd). */
+HPX_API int hpx_vsht_forward(hpx_plan_t plan, const void* map, void* alm, int64_t batch, int32_t csphase,
+                             void* workspace, size_t workspace_bytes, void* stream);
+HPX_API int hpx_vsht_inverse(hpx_plan_t plan, const void* alm, void* map, int64_t batch, int32_t csphase,
+                             void* workspace, size_t workspace_bytes, void* stream);
+HPX_API int hpx_vsht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_grad, int64_t batch,
+                                     int32_t csphase, void* workspace, size_t workspace_bytes, void* stream);
+HPX_API int hpx_vsht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch,
+                                     int32_t csphase, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Ragged batches: n_groups groups of maps, group g with its own plan (for
  * instance one plan per nside) transforming batches[g] contiguous maps
  * ins[g] -> outs[g], all in one call on one stream with one workspace of

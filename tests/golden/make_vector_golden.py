@@ -51,7 +51,14 @@ def case(hpx_sht, nside, L, M, csphase, seed):
     vi = hpx_sht.VectoriSHT(nside, lmax=L, mmax=M, csphase=csphase)
     alm = vs(torch.from_numpy(f)).numpy()
     vmap = vi(torch.from_numpy(a)).numpy()
-    return dict(f=f, alm=alm, a=a, map=vmap)
+    # autograd gradients of the reference: sum_lm |a_lm|^2 / (l+1) through
+    # VectorSHT, and sum f^2 through VectoriSHT
+    ft = torch.from_numpy(f).requires_grad_(True)
+    wl = 1.0 / (torch.arange(L, dtype=torch.float64) + 1.0)[:, None]
+    (vs(ft).abs() ** 2 * wl).sum().backward()
+    at = torch.from_numpy(a).requires_grad_(True)
+    (vi(at) ** 2).sum().backward()
+    return dict(f=f, alm=alm, a=a, map=vmap, grad_f=ft.grad.numpy(), grad_a=at.grad.numpy())
 
 
 def main(ref_root=None):
