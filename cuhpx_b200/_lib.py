@@ -64,6 +64,18 @@ class HpxDesc(ctypes.Structure):
     ]
 
 
+class HpxSchedule(ctypes.Structure):
+    _fields_ = [
+        ("ring_maps_per_cta", ctypes.c_int32),
+        ("fwd_deal", ctypes.c_int32),
+        ("inv_deal", ctypes.c_int32),
+        ("ctas", ctypes.c_int32),
+    ]
+
+
+DEALS = {"order_snake": 0, "tile_snake": 1, "greedy": 2, "contiguous": 3}
+
+
 class HpxStageStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char_p), ("launches", ctypes.c_int64), ("total_ms", ctypes.c_double)]
 
@@ -85,6 +97,8 @@ SIGNATURES = {
     "hpx_vsht_inverse": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_vsht_forward_adjoint": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
     "hpx_vsht_inverse_adjoint": ([_vp, _vp, _vp, _i64, ctypes.c_int32, _vp, _sz, _vp], ctypes.c_int),
+    "hpx_plan_get_schedule": ([_vp, ctypes.POINTER(HpxSchedule)], ctypes.c_int),
+    "hpx_plan_set_schedule": ([_vp, ctypes.POINTER(HpxSchedule)], ctypes.c_int),
     "hpx_plan_table_bytes": ([_vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hpx_plan_table_stream_bytes": ([_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz)], ctypes.c_int),
     "hpx_plan_create_latlon": ([ctypes.POINTER(HpxLatLonDesc), ctypes.POINTER(_vp)], ctypes.c_int),

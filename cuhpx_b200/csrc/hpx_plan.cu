@@ -121,6 +121,7 @@ struct hpx_plan_s {
     std::vector<int> h_lsmax;
     int n_fwdtiles = 0;
     float wmax = 0.f;            // largest ring weight w_t
+    int ring_g = 16;             // maps per ring-FFT CTA (hpx_plan_set_schedule)
     size_t ring_smem = 0, blue_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
@@ -290,34 +291,65 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// Assignment of tiles to at most `nsm` CTAs: tiles sorted by decreasing cost
-// (ties in list order, so a round holds neighbouring orders and CTAs working
-// at the same time share each order's data operand in L2) are dealt out in
-// rounds of one tile per CTA, alternating direction each round, which evens
-// the CTAs' sums.  Returns the CTA count; `order` receives the tiles grouped by
-// CTA (each in round order) and `off` the CTA boundaries.
-int schedule_tiles(const std::vector<int2>& tiles, const std::vector<double>& cost, int nsm, std::vector<int2>& order,
-                   std::vector<int>& off) {
+// Assignment of tiles to at most `nsm` CTAs (the m-to-CTA schedule of the
+// persistent tensor-core kernels).  `deal` picks the strategy
+// (HPX_DEAL_*):
+//   ORDER_SNAKE  tiles sorted by decreasing total cost of their order (ties in
+//                list order, so the tiles of one order stay together, are dealt
+//                to neighbouring CTAs in the same rounds and share the order's
+//                data operand in L2), dealt in rounds of one tile per CTA,
+//                alternating direction each round (balanced sums);
+//   TILE_SNAKE   the same rounds over tiles sorted by their own cost;
+//   GREEDY       longest tile first onto the least-loaded CTA;
+//   CONTIGUOUS   tiles in order sequence cut into ranges of equal cost, so a
+//                CTA keeps the tiles of few orders.
+// Returns the CTA count; `order` receives the tiles grouped by CTA and `off`
+// the CTA boundaries.
+int schedule_tiles(const std::vector<int2>& tiles, const std::vector<double>& cost, int nsm, int deal,
+                   std::vector<int2>& order, std::vector<int>& off) {
     const int n = (int)tiles.size();
     const int nc = std::max(1, std::min(nsm, n));
     std::vector<int> idx(n);
     for (int i = 0; i < n; ++i) idx[i] = i;
-    // sort by the total cost of the tile's order: the tiles of one order (m-major
-    // input, stable sort) stay together, are dealt to neighbouring CTAs in the
-    // same rounds and share the order's data operand in L2
-    std::vector<double> mcost(n);
-    for (int i = 0; i < n;) {
-        int j = i;
-        double c = 0.0;
-        while (j < n && tiles[j].x == tiles[i].x) c += cost[j++];
-        for (int k = i; k < j; ++k) mcost[k] = c;
-        i = j;
-    }
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return mcost[a] > mcost[b]; });
     std::vector<std::vector<int>> per(nc);
-    for (int k = 0; k < n; ++k) {
-        const int round = k / nc, pos = k % nc;
-        per[(round & 1) ? nc - 1 - pos : pos].push_back(idx[k]);
+    if (deal == HPX_DEAL_CONTIGUOUS) {
+        double total = 0.0;
+        for (double c : cost) total += c;
+        double acc = 0.0;
+        int cta = 0;
+        for (int i = 0; i < n; ++i) {
+            // move on once this CTA holds its share (keeping at least one tile for each later CTA)
+            if (cta < nc - 1 && acc >= total * (cta + 1) / nc && n - i > nc - 1 - cta) ++cta;
+            per[cta].push_back(i);
+            acc += cost[i];
+        }
+    } else {
+        if (deal == HPX_DEAL_TILE_SNAKE || deal == HPX_DEAL_GREEDY) {
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        } else {
+            std::vector<double> mcost(n);
+            for (int i = 0; i < n;) {
+                int j = i;
+                double c = 0.0;
+                while (j < n && tiles[j].x == tiles[i].x) c += cost[j++];
+                for (int k = i; k < j; ++k) mcost[k] = c;
+                i = j;
+            }
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return mcost[a] > mcost[b]; });
+        }
+        if (deal == HPX_DEAL_GREEDY) {
+            std::vector<double> load(nc, 0.0);
+            for (int k = 0; k < n; ++k) {
+                const int c = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+                per[c].push_back(idx[k]);
+                load[c] += cost[idx[k]];
+            }
+        } else {
+            for (int k = 0; k < n; ++k) {
+                const int round = k / nc, pos = k % nc;
+                per[(round & 1) ? nc - 1 - pos : pos].push_back(idx[k]);
+            }
+        }
     }
     order.clear();
     off.assign(1, 0);
@@ -339,6 +371,29 @@ int encode_table(const hpx_plan_s* P, CUtensorMap* map, int box_i, int box_rings
                                            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_err(HPX_ERR_CUDA, "cuTensorMapEncodeTiled (table) failed: " + std::to_string((int)r));
+    return HPX_OK;
+}
+
+// Deal the tensor-core tile lists onto the persistent CTAs with the given
+// strategies and CTA count (0: one per SM) and upload them (synchronous).
+int tc_deal(hpx_plan_s* P, int fwd_deal, int inv_deal, int ctas) {
+    TcPlan& T = P->tc;
+    const int nc = ctas > 0 ? std::min(ctas, T.nsm) : T.nsm;
+    std::vector<int2> order;
+    std::vector<int> off;
+    if (!T.fwd_list.empty()) {
+        T.n_fwd_ctas = schedule_tiles(T.fwd_list, T.fwd_cost, nc, fwd_deal, order, off);
+        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    }
+    if (!T.inv_list.empty()) {
+        T.n_inv_ctas = schedule_tiles(T.inv_list, T.inv_cost, nc, inv_deal, order, off);
+        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    }
+    T.fwd_deal = fwd_deal;
+    T.inv_deal = inv_deal;
+    T.ctas = ctas;
     return HPX_OK;
 }
 
@@ -468,22 +523,20 @@ int tc_create(hpx_plan_s* P) {
         for (int ci = nchI - ich[k]; ci < nchI; ++ci) c += t.x + ci * kTcDegChunk < P->h_lsmax[t.x] ? kSlow : 1.0;
         ic.push_back(c);
     }
-    std::vector<int2> order;
-    std::vector<int> off;
+    T.fwd_list = ft;
+    T.fwd_cost = fc;
+    T.inv_list = it;
+    T.inv_cost = ic;
     if (!ft.empty()) {
-        T.n_fwd_ctas = schedule_tiles(ft, fc, T.nsm, order, off);
-        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_tiles, sizeof(int2) * order.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
-        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_off, sizeof(int) * off.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_fwd_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_tiles, sizeof(int2) * ft.size()));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_fwd_off, sizeof(int) * (T.nsm + 1)));
     }
     if (!it.empty()) {
-        T.n_inv_ctas = schedule_tiles(it, ic, T.nsm, order, off);
-        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * order.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_tiles, order.data(), sizeof(int2) * order.size(), cudaMemcpyHostToDevice));
-        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_off, sizeof(int) * off.size()));
-        HPX_CUDA_TRY(cudaMemcpy(T.d_inv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_tiles, sizeof(int2) * it.size()));
+        HPX_CUDA_TRY(cudaMalloc(&T.d_inv_off, sizeof(int) * (T.nsm + 1)));
     }
+    const int rc_deal = tc_deal(P, HPX_DEAL_ORDER_SNAKE, HPX_DEAL_ORDER_SNAKE, 0);
+    if (rc_deal != HPX_OK) return rc_deal;
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_tc<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem));
@@ -933,10 +986,10 @@ struct Pipeline {
         }
     };
 
-    // maps per ring CTA: 16 amortise the CTA's table set-up (phase and twiddle
-    // tables, Bluestein chirp tables) over twice the maps of 8 (2.5% of the
-    // step); 32 measured no better
-    int maps_per_cta_ring() const { return 16; }
+    // maps per ring CTA (default 16: amortises the CTA's table set-up -- phase
+    // and twiddle tables, Bluestein chirp tables -- over twice the maps of 8,
+    // 2.5% of the step; 32 measured no better); set by hpx_plan_set_schedule
+    int maps_per_cta_ring() const { return P->ring_g; }
 
     // The power-of-two rings on the plan's auxiliary stream and the Bluestein
     // rings on st, forked and joined by events (valid under stream capture), so
@@ -1742,6 +1795,35 @@ int hpx_vsht_forward_adjoint(hpx_plan_t plan, const void* alm_grad, void* map_gr
 int hpx_vsht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_grad, int64_t batch, int32_t csphase,
                              void* ws, size_t ws_bytes, void* stream) {
     return dispatch_vec(plan, kInverseAdjoint, map_grad, alm_grad, batch, csphase, ws, ws_bytes, stream);
+}
+
+int hpx_plan_get_schedule(hpx_plan_t plan, hpx_schedule_t* s) {
+    if (!plan || !s) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    s->ring_maps_per_cta = plan->ring_g;
+    s->fwd_deal = plan->tc.fwd_deal;
+    s->inv_deal = plan->tc.inv_deal;
+    s->ctas = plan->tc.ctas;
+    return HPX_OK;
+}
+
+int hpx_plan_set_schedule(hpx_plan_t plan, const hpx_schedule_t* s) {
+    if (!plan || !s) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    const int g = s->ring_maps_per_cta;
+    if (g != 4 && g != 8 && g != 16 && g != 32) return set_err(HPX_ERR_INVALID_ARG, "ring_maps_per_cta must be 4, 8, 16 or 32");
+    for (int d : {s->fwd_deal, s->inv_deal})
+        if (d < HPX_DEAL_ORDER_SNAKE || d > HPX_DEAL_CONTIGUOUS) return set_err(HPX_ERR_INVALID_ARG, "unknown deal");
+    if (s->ctas < 0) return set_err(HPX_ERR_INVALID_ARG, "negative CTA count");
+    DeviceGuard g_(plan->device);
+    if (plan->tc.active) {
+        HPX_CUDA_TRY(cudaDeviceSynchronize());  // no launch of this plan may still read the old lists
+        const int rc = tc_deal(plan, s->fwd_deal, s->inv_deal, s->ctas);
+        if (rc != HPX_OK) return rc;
+    }
+    plan->tc.fwd_deal = s->fwd_deal;  // kept (and reported) for plans without tensor-core tiles too
+    plan->tc.inv_deal = s->inv_deal;
+    plan->tc.ctas = s->ctas;
+    plan->ring_g = g;
+    return HPX_OK;
 }
 
 int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes) {

@@ -50,7 +50,9 @@ __global__ void k_legendre_start(int M, int L, Geom geo, const RingPair* __restr
     int ls = L;
     double2 ps = make_double2(0.0, 0.0);
     const double s2 = pairs[p].s2;
-    if (m < L && p >= geo.first_ring(m) && (m == 0 || s2 > 0.0)) {  // poles carry m = 0 only
+    // rings from the first one that carries order m - 1: the spin-1 transforms
+    // of order m - 1 read Pbar^m there (the scalar ones start at first_ring(m))
+    if (m < L && p >= geo.first_ring(m > 0 ? m - 1 : 0) && (m == 0 || s2 > 0.0)) {  // poles carry m = 0 only
         const double x = pairs[p].z;
         const double lg = m == 0 ? logc[0] : logc[m] + 0.5 * (double)m * log2(s2);
         // scaled pair: value = mant * 2^E

@@ -41,6 +41,8 @@
 // to the plan's device flag and the kernel drains and returns.
 #pragma once
 
+#include <vector>
+
 #include "legendre.cuh"
 #include "tc_ptx.cuh"
 
@@ -170,6 +172,11 @@ struct TcPlan {
     CUtensorMap tab_fwd{}, tab_inv{};
     int Lh = 0;               // rows per (m, parity) of the synthesis operand
     void* encode = nullptr;   // cuTensorMapEncodeTiled (driver entry point)
+    // the tile lists in generation order and their costs, kept on the host so
+    // that a new schedule (hpx_plan_set_schedule) can deal them again
+    std::vector<int2> fwd_list, inv_list;
+    std::vector<double> fwd_cost, inv_cost;
+    int fwd_deal = 0, inv_deal = 0, ctas = 0;
 };
 
 // ------------------------------------------------------------------ shared layout

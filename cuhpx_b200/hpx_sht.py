@@ -24,7 +24,9 @@ Differences from the reference, all deliberate:
   or bf16 (~16-bit) split and FP32 accumulation),
   ``refine_iters`` (Jacobi refinement of the analysis), ``batch_chunk``,
   ``legendre_table`` (tensor-core plans: keep the Legendre values resident on
-  the device when they fit, default; False generates them on the fly).
+  the device when they fit, default; False generates them on the fly),
+  ``autotune`` (time the plan's launch schedules once and keep the fastest,
+  cached on disk: ``cuhpx_b200.autotune``).
 """
 
 import ctypes
@@ -283,7 +285,7 @@ def _device_index(x):
 
 class _Base(nn.Module):
     def __init__(self, nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
-                 legendre_table=True):
+                 legendre_table=True, autotune=False):
         super().__init__()
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA device is not available. This class requires a GPU.")
@@ -301,19 +303,26 @@ class _Base(nn.Module):
         self.refine_iters = int(refine_iters)
         self.batch_chunk = int(batch_chunk)
         self.legendre_table = bool(legendre_table)
+        self.autotune = bool(autotune)
         _lib.load()  # fail loudly at construction if the library is missing
 
     def _plan(self, dtype, device_index):
         prec = "fp64" if dtype == torch.float64 else self.precision
-        return get_plan(self.nside, self.lmax, self.mmax, self.quad_weights, prec, device_index, self.batch_chunk,
+        plan = get_plan(self.nside, self.lmax, self.mmax, self.quad_weights, prec, device_index, self.batch_chunk,
                         self.legendre_table)
+        if self.autotune and not getattr(plan, "_tuned", False):
+            from .autotune import tune
+
+            tune(plan, self.batch_chunk)
+            plan._tuned = True
+        return plan
 
 
 class SHTCUDA(_Base):
     def __init__(self, nside, lmax=None, mmax=None, quad_weights="ring", norm="ortho", csphase=True, *,
-                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True):
+                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True, autotune=False):
         super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
-                         legendre_table)
+                         legendre_table, autotune)
 
     def forward(self, x):
         if torch.is_complex(x):
@@ -331,9 +340,9 @@ class SHTCUDA(_Base):
 
 class iSHTCUDA(_Base):
     def __init__(self, nside, lmax=None, mmax=None, quad_weights="ring", norm="ortho", csphase=True, *,
-                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True):
+                 precision="fp32", refine_iters=0, batch_chunk=64, legendre_table=True, autotune=False):
         super().__init__(nside, lmax, mmax, quad_weights, norm, csphase, precision, refine_iters, batch_chunk,
-                         legendre_table)
+                         legendre_table, autotune)
 
     def forward(self, x):
         if not x.is_cuda:

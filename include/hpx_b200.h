@@ -218,6 +218,32 @@ typedef struct {
 } hpx_latlon_desc_t;
 HPX_API int hpx_plan_create_latlon(const hpx_latlon_desc_t* desc, hpx_plan_t* plan);
 
+/* Launch schedule of a plan (no counterpart in cuHPX, whose einsum and cuFFT
+ * calls have none): the autotuner of this library (cuhpx_b200/autotune.py)
+ * times candidates and keeps the fastest per GPU and problem.
+ *   ring_maps_per_cta  maps each ring-FFT CTA transforms (4, 8, 16 or 32; 16)
+ *   fwd_deal, inv_deal how the persistent tensor-core kernels' tiles are dealt
+ *                      to their CTAs (the m-to-CTA schedule), HPX_DEAL_*
+ *   ctas               persistent CTAs of those kernels (0: one per SM)
+ * hpx_plan_set_schedule synchronises the device and rewrites the plan's tile
+ * lists: call it while no transform of the plan is in flight and outside
+ * stream capture.  Every schedule gives bit-identical results: each tile and
+ * each ring transform is computed the same way whichever CTA runs it. */
+typedef enum {
+    HPX_DEAL_ORDER_SNAKE = 0,  /* orders by total cost, round-robin snake (default) */
+    HPX_DEAL_TILE_SNAKE = 1,   /* tiles by cost, round-robin snake               */
+    HPX_DEAL_GREEDY = 2,       /* longest tile first onto the least-loaded CTA    */
+    HPX_DEAL_CONTIGUOUS = 3    /* order sequence cut into equal-cost ranges       */
+} hpx_deal_t;
+typedef struct {
+    int32_t ring_maps_per_cta;
+    int32_t fwd_deal;
+    int32_t inv_deal;
+    int32_t ctas;
+} hpx_schedule_t;
+HPX_API int hpx_plan_get_schedule(hpx_plan_t plan, hpx_schedule_t* schedule);
+HPX_API int hpx_plan_set_schedule(hpx_plan_t plan, const hpx_schedule_t* schedule);
+
 /* Bytes of the plan's resident Legendre table (0 when it has none). */
 HPX_API int hpx_plan_table_bytes(hpx_plan_t plan, size_t* bytes);
 
