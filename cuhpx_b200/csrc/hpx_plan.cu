@@ -1715,6 +1715,14 @@ int hpx_workspace_size(hpx_plan_t plan, int64_t batch, size_t* bytes) {
     return HPX_OK;
 }
 
+// Ragged calls place the groups' workspaces one after another (256-byte
+// aligned) so that the groups can run at the same time on streams of their
+// own; a smaller workspace (at least the largest group's) runs them one after
+// another in it.
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+}  // namespace
+
 int hpx_ragged_workspace_size(const hpx_plan_t* plans, int32_t n_groups, const int64_t* batches, size_t* bytes) {
     if (!plans || !batches || !bytes || n_groups < 0) return set_err(HPX_ERR_INVALID_ARG, "null argument");
     size_t need = 0;
@@ -1722,28 +1730,95 @@ int hpx_ragged_workspace_size(const hpx_plan_t* plans, int32_t n_groups, const i
         if (!plans[g] || batches[g] < 0) return set_err(HPX_ERR_INVALID_ARG, "invalid group " + std::to_string(g));
         size_t b = 0;
         hpx_workspace_size(plans[g], batches[g], &b);
-        need = std::max(need, b);
+        need += align256(b);
     }
     *bytes = need;
     return HPX_OK;
 }
 
 namespace {
+// Streams and events the concurrent ragged groups fork onto, per device,
+// created on the first ragged call (make it outside stream capture) and kept
+// for the life of the process.
+constexpr int kRaggedStreams = 8;
+struct RaggedPool {
+    cudaStream_t s[kRaggedStreams] = {};
+    cudaEvent_t fork = nullptr, done[kRaggedStreams] = {};
+    bool ready = false;
+};
+std::mutex g_ragged_mu;
+RaggedPool g_ragged_pool[kNoAllocMaxDevices];
+
 int ragged(Op op, const hpx_plan_t* plans, int32_t n_groups, const void* const* ins, void* const* outs,
            const int64_t* batches, void* ws, size_t ws_bytes, void* stream) {
     if (!plans || !ins || !outs || !batches || n_groups < 0) return set_err(HPX_ERR_INVALID_ARG, "null argument");
+    size_t largest = 0, total = 0;
     for (int g = 0; g < n_groups; ++g) {
         if (!plans[g] || batches[g] < 0 || (batches[g] > 0 && (!ins[g] || !outs[g])))
             return set_err(HPX_ERR_INVALID_ARG, "invalid group " + std::to_string(g));
         if (plans[g]->device != plans[0]->device) return set_err(HPX_ERR_INVALID_ARG, "plans on different devices");
-        const int rc = check_call(plans[g], ins[g], outs[g], batches[g], ws, ws_bytes);
-        if (rc != HPX_OK) return rc;
+        size_t b = 0;
+        hpx_workspace_size(plans[g], batches[g], &b);
+        largest = std::max(largest, b);
+        total += align256(b);
     }
-    for (int g = 0; g < n_groups; ++g) {
-        const int rc = dispatch(plans[g], op, ins[g], outs[g], batches[g], ws, ws_bytes, stream);
-        if (rc != HPX_OK) return rc;
+    if (n_groups == 0) return HPX_OK;
+    if (!ws || ws_bytes < largest)
+        return set_err(HPX_ERR_WORKSPACE, "workspace too small: need " + std::to_string(total) + " bytes (at least " +
+                                              std::to_string(largest) + "), got " + std::to_string(ws_bytes));
+    if (((uintptr_t)ws & 255) != 0) return set_err(HPX_ERR_INVALID_ARG, "workspace must be 256-byte aligned");
+    int active = 0;
+    for (int g = 0; g < n_groups; ++g) active += batches[g] > 0;
+    if (ws_bytes < total || active < 2) {
+        for (int g = 0; g < n_groups; ++g) {
+            const int rc = dispatch(plans[g], op, ins[g], outs[g], batches[g], ws, ws_bytes, stream);
+            if (rc != HPX_OK) return rc;
+        }
+        return HPX_OK;
     }
-    return HPX_OK;
+    const int dev = plans[0]->device;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_err(HPX_ERR_UNSUPPORTED, "device ordinal above 63");
+    DeviceGuard dg(dev);
+    std::lock_guard<std::mutex> lk(g_ragged_mu);
+    RaggedPool& pool = g_ragged_pool[dev];
+    if (!pool.ready) {
+        for (int i = 0; i < kRaggedStreams; ++i) {
+            HPX_CUDA_TRY(cudaStreamCreateWithFlags(&pool.s[i], cudaStreamNonBlocking));
+            HPX_CUDA_TRY(cudaEventCreateWithFlags(&pool.done[i], cudaEventDisableTiming));
+        }
+        HPX_CUDA_TRY(cudaEventCreateWithFlags(&pool.fork, cudaEventDisableTiming));
+        pool.ready = true;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    HPX_CUDA_TRY(cudaEventRecord(pool.fork, st));
+    size_t off = 0;
+    int k = 0, rc = HPX_OK;
+    bool used[kRaggedStreams] = {};
+    for (int g = 0; g < n_groups && rc == HPX_OK; ++g) {
+        size_t b = 0;
+        hpx_workspace_size(plans[g], batches[g], &b);
+        if (batches[g] > 0) {
+            const int i = k++ % kRaggedStreams;
+            if (!used[i]) {
+                const cudaError_t e = cudaStreamWaitEvent(pool.s[i], pool.fork, 0);
+                if (e != cudaSuccess) {
+                    rc = set_err(HPX_ERR_CUDA, std::string("ragged fork: ") + cudaGetErrorString(e));
+                    break;
+                }
+                used[i] = true;
+            }
+            rc = dispatch(plans[g], op, ins[g], outs[g], batches[g], (char*)ws + off, align256(b), pool.s[i]);
+        }
+        off += align256(b);
+    }
+    // join every stream used (also after an error, so that no fork is left open)
+    for (int i = 0; i < kRaggedStreams; ++i) {
+        if (!used[i]) continue;
+        cudaError_t e = cudaEventRecord(pool.done[i], pool.s[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, pool.done[i], 0);
+        if (e != cudaSuccess && rc == HPX_OK) rc = set_err(HPX_ERR_CUDA, std::string("ragged join: ") + cudaGetErrorString(e));
+    }
+    return rc;
 }
 }  // namespace
 

@@ -2,9 +2,11 @@
 
 ``RaggedSHT(nsides, ...)(maps)`` analyses a list of map batches, one
 ``[B_g, 12 nside_g^2]`` tensor per resolution, through ``hpx_ragged_forward``
-(one library call, one stream, one shared workspace) and returns the list of
-``[B_g, L_g, M_g]`` coefficient tensors; ``RaggedISHT`` is the synthesis.  By
-default a group of resolution N keeps L = M = 2N - 1.
+(one library call; the groups run at the same time on streams the library
+forks from the current one) and returns the list of ``[B_g, L_g, M_g]``
+coefficient tensors; ``RaggedISHT`` is the synthesis.  By default a group of
+resolution N keeps L = M = 2N - 1.  ``autotune=True`` tunes each group's
+launch schedule for its batch size on the first call (``cuhpx_b200.autotune``).
 
 ``graph=True`` records the whole sequence of launches once in a CUDA graph
 (``torch.cuda.CUDAGraph``) for the batch sizes of the first call, and later
@@ -46,8 +48,9 @@ def split_by_offsets(flat, offsets, nsides):
 
 
 class _Ragged(nn.Module):
-    def __init__(self, nsides, lmax, mmax, precision, graph, legendre_table):
+    def __init__(self, nsides, lmax, mmax, precision, graph, legendre_table, autotune=False):
         super().__init__()
+        self.autotune = bool(autotune)
         self.nsides = [int(n) for n in nsides]
         self.lmax = [int(lmax(n)) if callable(lmax) else int(lmax or 2 * n - 1) for n in self.nsides]
         self.mmax = [int(mmax(n)) if callable(mmax) else int(mmax or 2 * n - 1) for n in self.nsides]
@@ -57,10 +60,18 @@ class _Ragged(nn.Module):
         self._g = None
         _lib.load()
 
-    def _plans(self, dtype, dev):
+    def _plans(self, dtype, dev, batches=None):
         prec = "fp64" if dtype in (torch.float64, torch.complex128) else self.precision
-        return [get_plan(n, L, M, "ring", prec, dev, 64, self.legendre_table)
-                for n, L, M in zip(self.nsides, self.lmax, self.mmax)]
+        plans = [get_plan(n, L, M, "ring", prec, dev, 64, self.legendre_table)
+                 for n, L, M in zip(self.nsides, self.lmax, self.mmax)]
+        if self.autotune and batches is not None:
+            from .autotune import tune
+
+            for p, b in zip(plans, batches):
+                if b > 0 and getattr(p, "_tuned_batch", None) != min(int(b), 64):
+                    tune(p, min(int(b), 64))
+                    p._tuned_batch = min(int(b), 64)
+        return plans
 
     def _run(self, fn, plans, ins, outs):
         lib = _lib.load()
@@ -104,13 +115,14 @@ class _Ragged(nn.Module):
 class RaggedSHT(_Ragged):
     """Analysis of a list of map batches of several resolutions (see module docstring)."""
 
-    def __init__(self, nsides, lmax=None, mmax=None, *, precision="fp32", graph=False, legendre_table=True):
-        super().__init__(nsides, lmax, mmax, precision, graph, legendre_table)
+    def __init__(self, nsides, lmax=None, mmax=None, *, precision="fp32", graph=False, legendre_table=True,
+                 autotune=False):
+        super().__init__(nsides, lmax, mmax, precision, graph, legendre_table, autotune)
 
     def _eager(self, xs):
         xs = [x.contiguous() for x in xs]
         dtype = xs[0].dtype
-        plans = self._plans(dtype, _device_index(xs[0]))
+        plans = self._plans(dtype, _device_index(xs[0]), [x.shape[0] for x in xs])
         cdt = torch.complex128 if dtype == torch.float64 else torch.complex64
         outs = [torch.empty((x.shape[0], L, M), dtype=cdt, device=x.device)
                 for x, L, M in zip(xs, self.lmax, self.mmax)]
@@ -124,13 +136,14 @@ class RaggedSHT(_Ragged):
 class RaggedISHT(_Ragged):
     """Synthesis of a list of coefficient batches of several resolutions."""
 
-    def __init__(self, nsides, lmax=None, mmax=None, *, precision="fp32", graph=False, legendre_table=True):
-        super().__init__(nsides, lmax, mmax, precision, graph, legendre_table)
+    def __init__(self, nsides, lmax=None, mmax=None, *, precision="fp32", graph=False, legendre_table=True,
+                 autotune=False):
+        super().__init__(nsides, lmax, mmax, precision, graph, legendre_table, autotune)
 
     def _eager(self, alms):
         alms = [a.resolve_conj().contiguous() for a in alms]
         dt = torch.float64 if alms[0].dtype == torch.complex128 else torch.float32
-        plans = self._plans(alms[0].dtype, _device_index(alms[0]))
+        plans = self._plans(alms[0].dtype, _device_index(alms[0]), [a.shape[0] for a in alms])
         outs = [torch.empty((a.shape[0], 12 * n * n), dtype=dt, device=a.device) for a, n in zip(alms, self.nsides)]
         self._ws = self._run(_lib.load().hpx_ragged_inverse, plans, [torch.view_as_real(a) for a in alms], outs)
         return outs

@@ -159,12 +159,17 @@ HPX_API int hpx_vsht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void
 
 /* Ragged batches: n_groups groups of maps, group g with its own plan (for
  * instance one plan per nside) transforming batches[g] contiguous maps
- * ins[g] -> outs[g], all in one call on one stream with one workspace of
- * hpx_ragged_workspace_size bytes (the groups run one after another and
- * reuse it).  Replaces a per-map loop over SHTCUDA objects; the sequence of
- * launches can be captured once in a CUDA graph.  An invalid group (null
- * plan or pointer, negative batch) fails the call before anything runs.
- * The plans must live on one device. */
+ * ins[g] -> outs[g], all in one call ordered on `stream`.  With a workspace
+ * of hpx_ragged_workspace_size bytes (the groups' workspaces one after
+ * another) the groups run at the same time on streams of the library's own,
+ * forked from `stream` and joined back to it by events (valid under stream
+ * capture; the library creates those streams on its first ragged call on a
+ * device, so make that call outside capture); with a smaller workspace of at
+ * least the largest group's size they run one after another in it.
+ * Replaces a per-map loop over SHTCUDA objects; the sequence of launches can
+ * be captured once in a CUDA graph.  An invalid group (null plan or pointer,
+ * negative batch) fails the call before anything runs.  The plans must live
+ * on one device. */
 HPX_API int hpx_ragged_workspace_size(const hpx_plan_t* plans, int32_t n_groups, const int64_t* batches,
                                       size_t* bytes);
 HPX_API int hpx_ragged_forward(const hpx_plan_t* plans, int32_t n_groups, const void* const* maps,
