@@ -98,3 +98,40 @@ def test_ragged_abi_errors(hpx, cuda):
     assert lib.hpx_ragged_workspace_size(ph1, 1, pb1, ctypes.byref(need)) == 0
     nul = (ctypes.c_void_p * 1)(None)
     assert lib.hpx_ragged_forward(ph1, 1, nul, nul, pb1, None, 0, None) == 1
+
+
+def test_ragged_concurrent_and_sequential_workspaces(hpx, cuda):
+    """The groups run concurrently when the workspace holds all of them (the size
+    hpx_ragged_workspace_size returns) and one after another in a workspace of the
+    largest group's size; both give the per-group results bit for bit."""
+    from cuhpx_b200 import _lib
+
+    lib = _lib.load()
+    rng = np.random.default_rng(6)
+    nsides, counts = [16, 8, 32, 8], [3, 2, 5, 1]  # two groups share a plan
+    maps = rand_maps(rng, nsides, counts, cuda)
+    plans = [hpx.get_plan(n, 2 * n - 1, 2 * n - 1, "ring", "f16x3", 0) for n in nsides]
+    outs = [torch.empty(c, 2 * n - 1, 2 * n - 1, dtype=torch.complex64, device=cuda) for n, c in zip(nsides, counts)]
+    k = len(nsides)
+    ph = (ctypes.c_void_p * k)(*[p._h.value for p in plans])
+    pi = (ctypes.c_void_p * k)(*[m.data_ptr() for m in maps])
+    po = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs])
+    pb = (ctypes.c_int64 * k)(*counts)
+    need = ctypes.c_size_t()
+    assert lib.hpx_ragged_workspace_size(ph, k, pb, ctypes.byref(need)) == 0
+    largest = max(p.workspace_bytes(c) for p, c in zip(plans, counts))
+    assert need.value >= sum(p.workspace_bytes(c) for p, c in zip(plans, counts)) > largest
+    refs = [hpx.SHTCUDA(n, lmax=2 * n - 1, mmax=2 * n - 1, precision="f16x3")(m) for n, m in zip(nsides, maps)]
+    stream = torch.cuda.current_stream(cuda).cuda_stream
+    for size in (need.value, largest):
+        ws = torch.empty(size + 256, dtype=torch.uint8, device=cuda)
+        base = (ws.data_ptr() + 255) & ~255
+        for o in outs:
+            o.fill_(float("nan"))
+        st = lib.hpx_ragged_forward(ph, k, pi, po, pb, base, size, stream)
+        assert st == 0, lib.hpx_last_error(None)
+        torch.cuda.synchronize()
+        for o, r in zip(outs, refs):
+            assert torch.equal(o, r), size
+    ws = torch.empty(largest - 256, dtype=torch.uint8, device=cuda)
+    assert lib.hpx_ragged_forward(ph, k, pi, po, pb, (ws.data_ptr() + 255) & ~255, largest - 512, stream) == 6
