@@ -747,11 +747,15 @@ def ragged_figures(torch, hpx, dev, prec, steps, warmup, loop_steps=2):
                         ("graph_analysis", replay_analysis, steps)):
         ms = time_steps(torch, fn, k, warmup if name != "loop" else 1, None, stream)
         res[name + "_maps_per_s"] = 96 * k / (ms / 1000.0)
+    # the graphs hold their inputs, outputs and workspaces: release them before
+    # the autotuned pair captures its own
+    del graphed, graphed_i, eager, eager_i
+    torch.cuda.empty_cache()
     # the same with each group's schedule autotuned for its batch (plans are
     # shared, so the fixed default is restored afterwards)
     from cuhpx_b200 import autotune as AT
 
-    plans = graphed._plans(torch.float32, dev.index)
+    plans = [hpx.get_plan(n, 2 * n - 1, 2 * n - 1, "ring", prec, dev.index) for n in nsides]
     saved = [AT.get_schedule(p) for p in plans]
     tuned_f = hpx.RaggedSHT(nsides, precision=prec, graph=True, autotune=True)
     tuned_i = hpx.RaggedISHT(nsides, precision=prec, graph=True, autotune=True)
@@ -763,6 +767,8 @@ def ragged_figures(torch, hpx, dev, prec, steps, warmup, loop_steps=2):
     ms = time_steps(torch, replay_tuned, steps, warmup, None, stream)
     res["graph_autotuned_maps_per_s"] = 96 * steps / (ms / 1000.0)
     res["autotuned_schedules"] = {str(n): AT.get_schedule(p) for n, p in zip(nsides, plans)}
+    del tuned_f, tuned_i
+    torch.cuda.empty_cache()
     for p, s0 in zip(plans, saved):
         AT.set_schedule(p, s0)
     return res

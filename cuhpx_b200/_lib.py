@@ -20,6 +20,7 @@ STATUS = {
     4: "timeout",
     5: "unsupported",
     6: "workspace too small",
+    7: "out-of-bounds access",
 }
 
 FLAG_OTF_LEGENDRE = 1

@@ -65,7 +65,7 @@ def build(force=False, debug=False, verbose=False, defines=(), out=None):
         target + ".tmp",
         *[os.path.join(CSRC, s) for s in SOURCES],
     ]
-    if debug:
+    if debug:  # the bounds-checked build (also VARIANTS["bounds"])
         cmd.insert(1, "-DHPX_CHECK_BOUNDS=1")
     for d in defines:
         cmd.insert(1, "-D" + d)
@@ -85,9 +85,13 @@ def build(force=False, debug=False, verbose=False, defines=(), out=None):
 #             kernels withhold their TMA loads, so their waits run out: the
 #             failure-detection test checks that a call then ends with
 #             HPX_ERR_TIMEOUT and leaves the device usable
+#   bounds    every global access of the ring, layout, contraction-epilogue and
+#             spin-1 kernels is checked against the call's buffer extents
+#             (skipped and reported as HPX_ERR_BOUNDS by hpx_plan_check)
 VARIANTS = {
     "waittest": (["HPX_WAIT_LIMIT_NS=1000000ull", "HPX_TEST_WITHHOLD_TMA_LOADS=1"],
                  os.path.join(HERE, "libhpx_b200_waittest.so")),
+    "bounds": (["HPX_CHECK_BOUNDS=1"], os.path.join(HERE, "libhpx_b200_bounds.so")),
 }
 
 

@@ -96,6 +96,31 @@ struct Geom {
     }
 };
 
+// ------------------------------------------------------------------ bounds-checked builds
+// Built with -DHPX_CHECK_BOUNDS (cuhpx_b200.build VARIANTS["bounds"]), the ring,
+// layout, contraction-epilogue and spin-1 kernels check the index of their
+// global accesses against the extents of the current chunk's buffers
+// (g_hpx_ext, written by the host before every chunk), skip any access outside
+// and record the first violation's code in g_hpx_oob; hpx_plan_check reports
+// it as HPX_ERR_BOUNDS.  Extents count elements from each buffer's base as the
+// kernels receive it: maps and ring spectra in real elements, coefficients in
+// real elements, ycols in floats, the synthesis operand in halves (per plane)
+// and the analysis operand in 32-bit words (per plane).  Without the define
+// every check is the constant true.
+enum HpxExtent { kExtMap = 0, kExtF, kExtSpec, kExtAlm, kExtYcols, kExtOperA, kExtOperX, kExtN };
+#ifdef HPX_CHECK_BOUNDS
+__device__ long long g_hpx_ext[kExtN];
+__device__ int g_hpx_oob;
+__device__ __forceinline__ bool hpx_inb(int64_t i, int ext, int code) {
+    if (i >= 0 && i < g_hpx_ext[ext]) return true;
+    atomicCAS(&g_hpx_oob, 0, code);
+    return false;
+}
+#define HPX_INB(i, ext, code) ::hpx::hpx_inb((int64_t)(i), (ext), (code))
+#else
+#define HPX_INB(i, ext, code) true
+#endif
+
 // ------------------------------------------------------------------ complex
 template <typename T>
 struct __align__(2 * sizeof(T)) cplx {

@@ -110,6 +110,10 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
+    // (bounds-checked builds) the CTA's first and last maps' ring and spectrum
+    if (b1 > b0 && !(HPX_INB(b0 * np + start, kExtMap, 1) && HPX_INB((b1 - 1) * np + start + 2 * rp.h - 1, kExtMap, 1) &&
+                     HPX_INB(2 * ((int64_t)(b1 - 1) * Ftot + foff + rp.mt) - 1, kExtF, 2)))
+        return;
     cplx<T>* cur = buf;
     cplx<T>* other = buf2;
     if (b0 + g < b1) ring_load_async(cur, map + (int64_t)(b0 + g) * np + start, rp.h, lt, tpf);
@@ -160,6 +164,9 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     const int64_t np = geo.npix;
     const int b0 = blockIdx.y * maps_per_cta;
     const int b1 = min(b0 + maps_per_cta, nmaps);
+    if (b1 > b0 && !(HPX_INB(b0 * np + start, kExtMap, 3) && HPX_INB((b1 - 1) * np + start + 2 * rp.h - 1, kExtMap, 3) &&
+                     HPX_INB(2 * ((int64_t)(b1 - 1) * Ftot + foff + rp.mt) - 1, kExtF, 4)))
+        return;
     cplx<T>* cur = buf;
     cplx<T>* other = buf2;
     auto spec = [&](int bb) { return (const cplx<T>*)(F + 2 * ((int64_t)bb * Ftot + foff)); };
@@ -238,8 +245,10 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
         vn[k] = {(T)0, (T)0};
         vs[k] = {(T)0, (T)0};
         if (b < nmaps && m < rp.mt) {
-            vn[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m));
-            if (rp.has_south) vs[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m));
+            if (HPX_INB(2 * ((int64_t)b * Ftot + rp.foff_n + m) + 1, kExtF, 5))
+                vn[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m));
+            if (rp.has_south && HPX_INB(2 * ((int64_t)b * Ftot + rp.foff_s + m) + 1, kExtF, 5))
+                vs[k] = *(const cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m));
         }
     }
     if (xh && fmax && tid < 64) {
@@ -272,6 +281,9 @@ __global__ void __launch_bounds__(256) k_fold(const T* __restrict__ F, int64_t F
         }
         const int64_t i0 = (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b;
         const int64_t i1 = (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b;
+        if (xh ? !(HPX_INB(i0 >> 1, kExtOperX, 6) && HPX_INB(i1 >> 1, kExtOperX, 6))
+               : !(HPX_INB(i0 + 1, kExtSpec, 6) && HPX_INB(i1 + 1, kExtSpec, 6)))
+            continue;
         if (xh && fmax) {
             const float sc = s_sc[bl];
             uint16_t h0, l0, h1, l1;
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int 
         const int mm = i >> 6, bl = i & 63, b = bz + bl, m = m0 + mm;
         ve[k] = {(T)0, (T)0};
         vo[k] = {(T)0, (T)0};
-        if (m < rp.mt && 2 * b < C) {
+        if (m < rp.mt && 2 * b < C && HPX_INB((((int64_t)m * 2 + 1) * NP + p) * C + 2 * b + 1, kExtSpec, 7)) {
             ve[k] = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 0) * NP + p) * C + 2 * b);
             vo[k] = *(const cplx<T>*)(spec + (((int64_t)m * 2 + 1) * NP + p) * C + 2 * b);
         }
@@ -344,8 +356,10 @@ __global__ void __launch_bounds__(256) k_unfold(const T* __restrict__ spec, int 
         T sc = (T)1;
         if (adjoint) sc = (m == 0 || m == rp.h) ? (T)rp.w : (T)(0.5 * rp.w);
         const cplx<T> e = te[mm][bl], o = to[mm][bl];
-        *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m)) = cscale(cadd(e, o), sc);
-        if (rp.has_south) *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m)) = cscale(csub(e, o), sc);
+        if (HPX_INB(2 * ((int64_t)b * Ftot + rp.foff_n + m) + 1, kExtF, 8))
+            *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_n + m)) = cscale(cadd(e, o), sc);
+        if (rp.has_south && HPX_INB(2 * ((int64_t)b * Ftot + rp.foff_s + m) + 1, kExtF, 8))
+            *(cplx<T>*)(F + 2 * ((int64_t)b * Ftot + rp.foff_s + m)) = cscale(csub(e, o), sc);
     }
 }
 

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -1144,6 +1145,35 @@ struct Pipeline {
 
 enum Op { kForward, kInverse, kForwardAdjoint, kInverseAdjoint, kForwardRefined };
 
+// Bounds-checked builds: the extents (elements from each buffer's base) of one
+// chunk's buffers, written before the chunk's launches on their stream.  The
+// failure-detection test shrinks one of them by an element
+// (HPX_TEST_SHRINK_EXTENT=<index>) so that the last access is reported (and
+// skipped).  In the product build this does nothing.
+void set_extents(const hpx_plan_s* P, cudaStream_t st, int64_t map_elems, int64_t alm_elems, int nb) {
+#ifdef HPX_CHECK_BOUNDS
+    long long v[kExtN];
+    v[kExtMap] = map_elems;
+    v[kExtF] = (long long)2 * nb * P->Ftot;
+    v[kExtSpec] = (long long)(P->spec_bytes() / P->real_size());
+    v[kExtAlm] = alm_elems;
+    v[kExtYcols] = (long long)(P->ycols_bytes() / sizeof(float));
+    v[kExtOperA] = P->mixed() ? (long long)2 * P->M * P->tc.Lh * kTcCols : 0;
+    v[kExtOperX] = P->mixed() ? (long long)2 * P->M * P->NP * kTcCols / 2 : 0;
+    if (const char* e = getenv("HPX_TEST_SHRINK_EXTENT")) {
+        const int k = atoi(e);
+        if (k >= 0 && k < kExtN && v[k] > 0) v[k] -= 1;
+    }
+    cudaMemcpyToSymbolAsync(g_hpx_ext, v, sizeof(v), 0, cudaMemcpyHostToDevice, st);
+#else
+    (void)P;
+    (void)st;
+    (void)map_elems;
+    (void)alm_elems;
+    (void)nb;
+#endif
+}
+
 // Spin-1 transforms of a plan built with L+1 degrees and M+1 orders (see
 // vector.cuh): maps [batch][2][npix] <-> coefficients [batch][2][L][M].  Each
 // pass takes batch_chunk / 2 vector maps, whose 2 components run through the
@@ -1158,6 +1188,7 @@ int run_vec(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void
     const size_t map_stride = (size_t)2 * P->npix;
     for (int64_t b0 = 0; b0 < batch; b0 += vc) {
         const int nb = (int)std::min<int64_t>(vc, batch - b0);
+        set_extents(P, st, (int64_t)nb * map_stride, (int64_t)nb * alm_stride, 2 * nb);
         const bool analysis = op == kForward || op == kInverseAdjoint;
         if (analysis) {
             const T* map = (const T*)in + b0 * map_stride;
@@ -1215,6 +1246,7 @@ int run_op(hpx_plan_s* P, Op op, const void* in, void* out, int64_t batch, void*
     const size_t alm_stride = (size_t)P->L * P->M * 2;
     for (int64_t b0 = 0; b0 < batch; b0 += bc) {
         const int nb = (int)std::min<int64_t>(bc, batch - b0);
+        set_extents(P, st, (int64_t)nb * P->npix, (int64_t)nb * alm_stride, nb);
         switch (op) {
             case kForward:
             case kInverseAdjoint: {
@@ -1364,6 +1396,7 @@ int run_forward_noalloc(hpx_plan_s* P, const void* in, void* out, int64_t batch,
     const size_t alm_stride = (size_t)P->L * P->M * 2;
     for (int64_t b0 = 0; b0 < batch; b0 += bc) {
         const int nb = (int)std::min<int64_t>(bc, batch - b0);
+        set_extents(P, st, (int64_t)nb * P->npix, (int64_t)nb * alm_stride, nb);
         pl.ring_fwd((const T*)in + b0 * P->npix, nb, 0);
         pl.leg_fwd((T*)out + b0 * alm_stride, nb, 0);
         if (pl.rc != HPX_OK) return pl.rc;
@@ -1916,8 +1949,20 @@ int hpx_plan_table_stream_bytes(hpx_plan_t plan, size_t* fwd, size_t* inv) {
 
 int hpx_plan_check(hpx_plan_t plan, void* stream) {
     if (!plan) return set_err(HPX_ERR_INVALID_ARG, "null plan");
-    if (!plan->tc.d_err) return HPX_OK;
     DeviceGuard dg(plan->device);
+#ifdef HPX_CHECK_BOUNDS
+    {
+        HPX_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+        int oob = 0;
+        HPX_CUDA_TRY(cudaMemcpyFromSymbol(&oob, g_hpx_oob, sizeof(int)));
+        if (oob != 0) {
+            const int zero = 0;
+            cudaMemcpyToSymbol(g_hpx_oob, &zero, sizeof(int));
+            return set_err(HPX_ERR_BOUNDS, "out-of-bounds access skipped (site code " + std::to_string(oob) + ")");
+        }
+    }
+#endif
+    if (!plan->tc.d_err) return HPX_OK;
     int h = 0;
     HPX_CUDA_TRY(cudaMemcpyAsync(&h, plan->tc.d_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     HPX_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
@@ -1990,6 +2035,7 @@ const char* hpx_status_string(int status) {
         case HPX_ERR_TIMEOUT: return "timeout";
         case HPX_ERR_UNSUPPORTED: return "unsupported";
         case HPX_ERR_WORKSPACE: return "workspace too small";
+        case HPX_ERR_BOUNDS: return "out-of-bounds access";
         default: return "unknown status";
     }
 }

@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(256) k_leg_fwd_simt(const T* __restrict__ spec
         for (int cc = 0; cc < 8; cc += 2) {
             const int c = c0 + (cc < 4 ? cA + cc : cB + cc - 4);
             const int b = c >> 1;
-            if (b < nmaps) {
+            if (b < nmaps && HPX_INB(2 * (((int64_t)b * L + l) * M + m) + 1, kExtAlm, 15)) {
                 cplx<T>* dst = (cplx<T>*)(alm + 2 * (((int64_t)b * L + l) * M + m));
                 cplx<T> v = {acc[i][cc], acc[i][cc + 1]};
                 if (accumulate) v = cadd(*dst, v);
@@ -490,7 +490,8 @@ __global__ void __launch_bounds__(256) k_leg_inv_simt(const T* __restrict__ almT
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int r = rb + rrow + i;
-        if (r >= K) continue;
+        if (r >= K || !HPX_INB((((int64_t)m * 2 + 1) * NP + t0 + r) * C + c0 + min(CT, C - c0) - 1, kExtSpec, 16))
+            continue;
         T* e = spec + (((int64_t)m * 2 + 0) * NP + t0 + r) * C + c0;
         T* o = spec + (((int64_t)m * 2 + 1) * NP + t0 + r) * C + c0;
 #pragma unroll

@@ -629,9 +629,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         const int lr0 = l0 + 2 * ew * 32 + par;  // degree of row 0 of this warp
                         epi_store_block(stg, v, lane, [&](int r) -> float* {
                             const int lr = lr0 + 2 * r;
-                            return lr < L ? ycols + ((int64_t)m * L + lr) * kTcCols + c : nullptr;
+                            return (lr < L && HPX_INB(((int64_t)m * L + lr) * kTcCols + c + 15, kExtYcols, 13))
+                                       ? ycols + ((int64_t)m * L + lr) * kTcCols + c
+                                       : nullptr;
                         });
-                    } else if (l < L) {
+                    } else if (l < L && HPX_INB(((int64_t)m * L + l) * kTcCols + c + 15, kExtYcols, 13)) {
                         float* dst = ycols + ((int64_t)m * L + l) * kTcCols + c;
 #pragma unroll
                         for (int j = 0; j < 16; j += 4) {
@@ -943,7 +945,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             tc::tma_store_3d(&spec_map, stg, c, t0 + rb + ew * 32, 2 * m + par);
                             tc::bulk_commit();
                         }
-                    } else if (p < NP && c < C) {
+                    } else if (p < NP && c < C && HPX_INB(dst - spec + c + 15, kExtSpec, 14)) {
 #pragma unroll
                         for (int j = 0; j < 16; j += 4) {
                             const float s0 = s_inv[(c + j) >> 1], s1 = s_inv[((c + j) >> 1) + 1];
@@ -1097,7 +1099,8 @@ __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int
     for (int k = 0; k < 8; ++k) {
         const int i = ty + 8 * k, m = m0 + tx;
         vv[k] = make_float2(0.f, 0.f);
-        if (i < nmaps && m < M && m <= l && l < L) vv[k] = *(const float2*)(alm + 2 * (((int64_t)i * L + l) * M + m));
+        if (i < nmaps && m < M && m <= l && l < L && HPX_INB(2 * (((int64_t)i * L + l) * M + m) + 1, kExtAlm, 9))
+            vv[k] = *(const float2*)(alm + 2 * (((int64_t)i * L + l) * M + m));
     }
     if (amax && ty < 2) {
         const int b = ty * 32 + tx;
@@ -1111,7 +1114,7 @@ __global__ void k_alm_to_tc(const float* __restrict__ alm, int nmaps, int L, int
         const int m = m0 + mi;
         if (m >= M || l < m) continue;
         const int d = l - m, par = d & 1, i = d >> 1;
-        if (i >= Lh) continue;
+        if (i >= Lh || !HPX_INB((((int64_t)(2 * m + par)) * Lh + i) * kTcCols + kTcCols - 1, kExtOperA, 10)) continue;
         uint32_t* rh = (uint32_t*)(ah + (((int64_t)(2 * m + par)) * Lh + i) * kTcCols);
         uint32_t* rl = (uint32_t*)(al + (((int64_t)(2 * m + par)) * Lh + i) * kTcCols);
         for (int b = tx; b < 64; b += 32) {
@@ -1146,7 +1149,7 @@ __global__ void k_tc_to_alm(const float* __restrict__ ycols, int nmaps, int L, i
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int m = m0 + ty + 8 * k;
-        const bool live = m < m_end && m <= l;
+        const bool live = m < m_end && m <= l && HPX_INB(((int64_t)m * L + l) * kTcCols + kTcCols - 1, kExtYcols, 11);
         const float2* row = (const float2*)(ycols + ((int64_t)m * L + l) * kTcCols);
 #pragma unroll
         for (int h = 0; h < 2; ++h) vv[k][h] = live ? row[tx + 32 * h] : make_float2(0.f, 0.f);
@@ -1159,6 +1162,7 @@ __global__ void k_tc_to_alm(const float* __restrict__ ycols, int nmaps, int L, i
     const int m = m0 + tx;
     if (m >= m_end) return;
     for (int b = ty; b < nmaps && b < 64; b += 8) {
+        if (!HPX_INB(2 * (((int64_t)b * L + l) * M + m) + 1, kExtAlm, 12)) continue;
         float2* dst = (float2*)(alm + 2 * (((int64_t)b * L + l) * M + m));
         float2 v = tile[b][tx];
         if (accumulate) {

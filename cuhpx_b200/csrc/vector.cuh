@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(256) k_vleg_fwd(const T* __restrict__ spec, in
         const int lz = min(m, Lv);
         for (int i = tid; i < lz * (CT / 4) * 2; i += blockDim.x) {
             const int comp = i & 1, vb = vb0 + (i >> 1) % (CT / 4), l = (i >> 1) / (CT / 4);
-            if (vb < nvec) *(cplx<T>*)(alm + 2 * ((((int64_t)vb * 2 + comp) * Lv + l) * Mv + m)) = {(T)0, (T)0};
+            if (vb < nvec && HPX_INB(2 * ((((int64_t)vb * 2 + comp) * Lv + l) * Mv + m) + 1, kExtAlm, 17))
+                *(cplx<T>*)(alm + 2 * ((((int64_t)vb * 2 + comp) * Lv + l) * Mv + m)) = {(T)0, (T)0};
         }
     }
     if (m >= Lv || l0 >= Lv) return;
@@ -274,6 +275,7 @@ __global__ void __launch_bounds__(256) k_vleg_fwd(const T* __restrict__ spec, in
         if (l >= Lv) continue;
         T nf = (l == 0 || !use_nf) ? (T)1 : (T)(1.0 / ((double)l * (double)(l + 1)));
         if (csphase && (m & 1)) nf = -nf;
+        if (!HPX_INB(2 * ((((int64_t)vb * 2 + 1) * Lv + l) * Mv + m) + 1, kExtAlm, 18)) continue;
         const cplx<T> S = {nf * (A[i][0] + B[i][3]), nf * (A[i][1] - B[i][2])};
         const cplx<T> Tt = {nf * (B[i][1] - A[i][2]), -nf * (A[i][3] + B[i][0])};
         *(cplx<T>*)(alm + 2 * ((((int64_t)vb * 2 + 0) * Lv + l) * Mv + m)) = S;
@@ -417,7 +419,8 @@ __global__ void __launch_bounds__(256) k_vleg_inv(const T* __restrict__ alm, int
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int r = rb + rrow + i;
-        if (r >= K) continue;
+        if (r >= K || c0 + 4 * tx >= C || !HPX_INB((((int64_t)m * 2 + 1) * NP + t0 + r) * C + c0 + 4 * tx + 3, kExtSpec, 19))
+            continue;
         T* e = spec + (((int64_t)m * 2 + 0) * NP + t0 + r) * C + c0 + 4 * tx;
         T* o = spec + (((int64_t)m * 2 + 1) * NP + t0 + r) * C + c0 + 4 * tx;
 #pragma unroll

@@ -88,6 +88,13 @@ class _Ragged(nn.Module):
         _lib.check(fn(ph, n, pi, po, pb, ctypes.c_void_p(ws.data_ptr()), need.value, ctypes.c_void_p(stream)))
         return ws
 
+    def _keep(self, ws):
+        # A captured graph reads its workspace at every replay, so graph mode
+        # keeps it; an eager call may release it at once: the library joins
+        # its group streams back into the caller's stream before returning,
+        # so the allocator's stream-ordered reuse comes after the last kernel.
+        self._ws = ws if self.graph else None
+
     def _call(self, xs):
         if len(xs) != len(self.nsides):
             raise ValueError(f"expected {len(self.nsides)} groups, got {len(xs)}")
@@ -126,7 +133,8 @@ class RaggedSHT(_Ragged):
         cdt = torch.complex128 if dtype == torch.float64 else torch.complex64
         outs = [torch.empty((x.shape[0], L, M), dtype=cdt, device=x.device)
                 for x, L, M in zip(xs, self.lmax, self.mmax)]
-        self._ws = self._run(_lib.load().hpx_ragged_forward, plans, xs, [torch.view_as_real(o) for o in outs])
+        ws = self._run(_lib.load().hpx_ragged_forward, plans, xs, [torch.view_as_real(o) for o in outs])
+        self._keep(ws)
         return outs
 
     def forward(self, maps):
@@ -145,7 +153,8 @@ class RaggedISHT(_Ragged):
         dt = torch.float64 if alms[0].dtype == torch.complex128 else torch.float32
         plans = self._plans(alms[0].dtype, _device_index(alms[0]), [a.shape[0] for a in alms])
         outs = [torch.empty((a.shape[0], 12 * n * n), dtype=dt, device=a.device) for a, n in zip(alms, self.nsides)]
-        self._ws = self._run(_lib.load().hpx_ragged_inverse, plans, [torch.view_as_real(a) for a in alms], outs)
+        ws = self._run(_lib.load().hpx_ragged_inverse, plans, [torch.view_as_real(a) for a in alms], outs)
+        self._keep(ws)
         return outs
 
     def forward(self, alms):

@@ -48,7 +48,8 @@ typedef enum {
     HPX_ERR_CUDA = 3,
     HPX_ERR_TIMEOUT = 4,
     HPX_ERR_UNSUPPORTED = 5,
-    HPX_ERR_WORKSPACE = 6
+    HPX_ERR_WORKSPACE = 6,
+    HPX_ERR_BOUNDS = 7   /* bounds-checked debug builds only: an access outside a buffer was skipped */
 } hpx_status_t;
 
 /* Arithmetic of the Legendre contraction.  FFT stages run in float for
@@ -193,7 +194,9 @@ HPX_API int hpx_stats_enable(hpx_plan_t plan, int enable);
 HPX_API int hpx_stats_read(hpx_plan_t plan, hpx_stage_stat_t* out, int max_stages, int* n_stages);
 
 /* Synchronise `stream` and report whether a kernel of this plan gave up on a
- * bounded pipeline wait since the last check (HPX_ERR_TIMEOUT, flag cleared). */
+ * bounded pipeline wait since the last check (HPX_ERR_TIMEOUT, flag cleared).
+ * Bounds-checked builds (-DHPX_CHECK_BOUNDS) also report, first, an access
+ * outside the current call's buffers that a kernel skipped (HPX_ERR_BOUNDS). */
 HPX_API int hpx_plan_check(hpx_plan_t plan, void* stream);
 
 /* Latitude-longitude grids (the destination side of cuHPX's Regridding,
