@@ -71,6 +71,7 @@ class HpxSchedule(ctypes.Structure):
         ("fwd_deal", ctypes.c_int32),
         ("inv_deal", ctypes.c_int32),
         ("ctas", ctypes.c_int32),
+        ("ring_streams", ctypes.c_int32),
     ]
 
 

@@ -2,11 +2,12 @@
 
 For one plan and batch size it times candidate schedules on random maps of
 the plan's shape, on the device, and keeps the fastest: the maps each
-ring-FFT CTA transforms (4, 8, 16, 32), and, for tensor-core plans, how the
+ring-FFT CTA transforms (4, 8, 16, 32), whether the power-of-two and the
+Bluestein ring launches overlap on two streams, and, for tensor-core plans, how the
 analysis and the synthesis tiles are dealt to the persistent CTAs (the
 m-to-CTA schedule: ``order_snake``, ``tile_snake``, ``greedy``,
-``contiguous``).  The search is coordinate-wise: ring grouping on the whole
-SHT + iSHT step, then the analysis deal on the analysis, then the synthesis
+``contiguous``).  The search is coordinate-wise: ring grouping and ring
+streams on the whole SHT + iSHT step, then the analysis deal on the analysis, then the synthesis
 deal on the synthesis; each candidate is the median of ``reps`` CUDA-event
 timings after ``warmup`` calls.  Results are cached in a JSON file keyed by
 GPU name, nside, lmax, mmax, batch, precision and whether the plan holds the
@@ -57,7 +58,7 @@ def get_schedule(plan):
     _lib.check(plan._lib.hpx_plan_get_schedule(plan._h, s), plan._h)
     inv = {v: k for k, v in _lib.DEALS.items()}
     return {"ring_maps_per_cta": s.ring_maps_per_cta, "fwd_deal": inv[s.fwd_deal], "inv_deal": inv[s.inv_deal],
-            "ctas": s.ctas}
+            "ctas": s.ctas, "ring_streams": s.ring_streams}
 
 
 def set_schedule(plan, sched):
@@ -66,6 +67,7 @@ def set_schedule(plan, sched):
     s.fwd_deal = _lib.DEALS[sched["fwd_deal"]]
     s.inv_deal = _lib.DEALS[sched["inv_deal"]]
     s.ctas = int(sched.get("ctas", 0))
+    s.ring_streams = int(sched.get("ring_streams", 2))
     _lib.check(plan._lib.hpx_plan_set_schedule(plan._h, s), plan._h)
 
 
@@ -130,6 +132,8 @@ def tune(plan, batch, warmup=2, reps=3, cache=True, force=False):
         with torch.no_grad():
             tc = plan.precision in ("f16x3", "bf16x3")
             cands = [(f"ring_maps_per_cta={gsz}", dict(best, ring_maps_per_cta=gsz)) for gsz in RING_GROUPS]
+            best = min(cands, key=lambda c: trial(c[0], c[1], step))[1]
+            cands = [(f"ring_streams={k}", dict(best, ring_streams=k)) for k in (2, 1)]
             best = min(cands, key=lambda c: trial(c[0], c[1], step))[1]
             if tc:
                 cands = [(f"fwd_deal={d}", dict(best, fwd_deal=d)) for d in DEALS]

@@ -123,6 +123,7 @@ struct hpx_plan_s {
     int n_fwdtiles = 0;
     float wmax = 0.f;            // largest ring weight w_t
     int ring_g = 16;             // maps per ring-FFT CTA (hpx_plan_set_schedule)
+    int ring_streams = 2;        // 2: ring launches overlap on the aux stream; 1: serial
     size_t ring_smem = 0, blue_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
@@ -997,7 +998,7 @@ struct Pipeline {
     // that the two launches and their tails overlap.
     template <typename Pow2, typename Blue>
     void ring_launches(Pow2 pow2, Blue blue) {
-        if (P->n_rings_pow2 && P->n_rings_blue) {
+        if (P->n_rings_pow2 && P->n_rings_blue && P->ring_streams == 2) {
             std::lock_guard<std::mutex> lk(P->fork_mu);
             cudaError_t e = cudaEventRecord(P->ev_fork, st);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(P->aux, P->ev_fork, 0);
@@ -1908,6 +1909,7 @@ int hpx_vsht_inverse_adjoint(hpx_plan_t plan, const void* map_grad, void* alm_gr
 int hpx_plan_get_schedule(hpx_plan_t plan, hpx_schedule_t* s) {
     if (!plan || !s) return set_err(HPX_ERR_INVALID_ARG, "null argument");
     s->ring_maps_per_cta = plan->ring_g;
+    s->ring_streams = plan->ring_streams;
     s->fwd_deal = plan->tc.fwd_deal;
     s->inv_deal = plan->tc.inv_deal;
     s->ctas = plan->tc.ctas;
@@ -1921,6 +1923,7 @@ int hpx_plan_set_schedule(hpx_plan_t plan, const hpx_schedule_t* s) {
     for (int d : {s->fwd_deal, s->inv_deal})
         if (d < HPX_DEAL_ORDER_SNAKE || d > HPX_DEAL_CONTIGUOUS) return set_err(HPX_ERR_INVALID_ARG, "unknown deal");
     if (s->ctas < 0) return set_err(HPX_ERR_INVALID_ARG, "negative CTA count");
+    if (s->ring_streams != 1 && s->ring_streams != 2) return set_err(HPX_ERR_INVALID_ARG, "ring_streams must be 1 or 2");
     DeviceGuard g_(plan->device);
     if (plan->tc.active) {
         HPX_CUDA_TRY(cudaDeviceSynchronize());  // no launch of this plan may still read the old lists
@@ -1931,6 +1934,7 @@ int hpx_plan_set_schedule(hpx_plan_t plan, const hpx_schedule_t* s) {
     plan->tc.inv_deal = s->inv_deal;
     plan->tc.ctas = s->ctas;
     plan->ring_g = g;
+    plan->ring_streams = s->ring_streams;
     return HPX_OK;
 }
 

@@ -233,6 +233,7 @@ HPX_API int hpx_plan_create_latlon(const hpx_latlon_desc_t* desc, hpx_plan_t* pl
  *   fwd_deal, inv_deal how the persistent tensor-core kernels' tiles are dealt
  *                      to their CTAs (the m-to-CTA schedule), HPX_DEAL_*
  *   ctas               persistent CTAs of those kernels (0: one per SM)
+ *   ring_streams       2 (default) or 1, see the field
  * hpx_plan_set_schedule synchronises the device and rewrites the plan's tile
  * lists: call it while no transform of the plan is in flight and outside
  * stream capture.  Every schedule gives bit-identical results: each tile and
@@ -248,6 +249,8 @@ typedef struct {
     int32_t fwd_deal;
     int32_t inv_deal;
     int32_t ctas;
+    int32_t ring_streams;  /* 2: the power-of-two and Bluestein ring launches overlap on two
+                              streams (default); 1: they run one after the other on the call's stream */
 } hpx_schedule_t;
 HPX_API int hpx_plan_get_schedule(hpx_plan_t plan, hpx_schedule_t* schedule);
 HPX_API int hpx_plan_set_schedule(hpx_plan_t plan, const hpx_schedule_t* schedule);

@@ -30,15 +30,16 @@ def test_every_schedule_is_bit_identical(hpx, cuda, prec):
     g = torch.Generator(device=cuda).manual_seed(3)
     x = torch.randn(70, 12 * nside * nside, generator=g, device=cuda)
     default = AT.get_schedule(plan)
-    assert default == {"ring_maps_per_cta": 16, "fwd_deal": "order_snake", "inv_deal": "order_snake", "ctas": 0}
+    assert default == {"ring_maps_per_cta": 16, "fwd_deal": "order_snake", "inv_deal": "order_snake", "ctas": 0,
+                       "ring_streams": 2}
     ref_a = plan.forward(x)
     ref_f = plan.inverse(ref_a)
     deals = AT.DEALS if prec == "f16x3" else ("order_snake",)
     try:
         for gsz in AT.RING_GROUPS:
             for d in deals:
-                for ctas in (0, 37):
-                    s = {"ring_maps_per_cta": gsz, "fwd_deal": d, "inv_deal": d, "ctas": ctas}
+                for ctas, rs in ((0, 2), (37, 1)):
+                    s = {"ring_maps_per_cta": gsz, "fwd_deal": d, "inv_deal": d, "ctas": ctas, "ring_streams": rs}
                     AT.set_schedule(plan, s)
                     assert AT.get_schedule(plan) == s
                     a = plan.forward(x)
@@ -60,8 +61,8 @@ def test_autotune_caches_and_reapplies(hpx, cuda, tmp_path, monkeypatch):
     try:
         r = AT.tune(plan, 64, warmup=1, reps=2)
         assert not r["cached"]
-        # every candidate was timed: 4 ring groupings and 4 deals in each direction
-        assert len(r["ms"]) == 12 and all(v > 0 for v in r["ms"].values())
+        # every candidate was timed: 4 ring groupings, 2 ring-stream modes and 4 deals in each direction
+        assert len(r["ms"]) == 14 and all(v > 0 for v in r["ms"].values())
         assert AT.get_schedule(plan) == r["schedule"]
         data = json.loads((tmp_path / "schedules.json").read_text())
         assert AT.key(plan, 64) in data
