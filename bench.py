@@ -329,7 +329,7 @@ def run_gpu(args):
         raise RuntimeError(f"timed transform disagrees with the FP32 path: rel-L2 {check_rel:.3e}")
     ms_step = ms / args.steps
     value = world * B * args.steps / (ms / 1000.0)
-    launches_per_step = sum(v[0] * kernels_in_stage(k, prec) for k, v in stats.items()) / args.steps
+    launches_per_step = sum(v[0] * kernels_in_stage(k, prec, nside) for k, v in stats.items()) / args.steps
 
     # roofline of the dominant kernel
     roof = roofline(stats, args, prec, refine, nside, L, B, plan.table_bytes > 0, plan.table_stream_bytes)
@@ -625,13 +625,27 @@ MEASURED_TRAFFIC = {
     "unfold": 3252765440 + 3185650688,
 }
 
-# kernels behind each stage's timer: the ring stages launch the power-of-two
-# rings and the Bluestein rings as two kernels (HEALPix grids have both), and
-# the mixed path's alm_to_columns is a max scan plus the conversion when the
-# operand carries a per-map fp16 scale
-def kernels_in_stage(name, prec):
+def ring_kernel_count(nside):
+    """Kernels of a ring stage: one per ring list the plan has -- power-of-two
+    rings, Bluestein rings of length 2^K, Bluestein rings of length 3072 (for
+    2h - 1 in (2048, 3072], nside <= 1024) -- for the rings' h = 2i (polar
+    ring i) and 2 nside (equatorial rings)."""
+    kinds = set()
+    for h in list(range(2, 2 * nside, 2)) + [2 * nside]:
+        if h & (h - 1) == 0:
+            kinds.add(0)
+        else:
+            p2 = 1 << (2 * h - 2).bit_length()
+            kinds.add(2 if (nside <= 1024 and 2 * h - 1 <= 3072 < p2) else 1)
+    return len(kinds)
+
+
+# kernels behind each stage's timer: the ring stages launch one kernel per ring
+# list, and the mixed path's alm_to_columns is a max scan plus the conversion
+# when the operand carries a per-map fp16 scale
+def kernels_in_stage(name, prec, nside):
     if name.startswith("ring_fft"):
-        return 2
+        return ring_kernel_count(nside)
     return 2 if (name == "alm_to_columns" and prec == "f16x3") else 1
 
 

@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(256) k_ring_tables(const RingPair* __restrict_
     const RingPair rp = pairs[blockIdx.x];
     cplx<T>* et = out + (size_t)blockIdx.x * slot;
     build_phase_tab(et, rp.nphi);
-    if (rp.logP > 0) build_phase_tab(et + phase_tab_elems(rp.nphi), (1 << rp.logP) / 2);
+    if (rp.logP > 0) build_phase_tab(et + phase_tab_elems(rp.nphi), ring_fft_len(rp) / 2);
 }
 
 // complex elements of a ring pair's table slot (nmax: the largest nphi)
@@ -39,12 +39,12 @@ __host__ __device__ constexpr int ring_table_slot(int pfft_max, int nmax) {
 
 // shared-memory layout of a ring CTA: phase table E, FFT twiddles (copied from
 // the pair's slot), then the work buffers
-template <typename T>
+template <int KIND, typename T>
 __device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingPair& rp,
                                                 const cplx<T>* __restrict__ slot, PhaseTab<T>& E, PhaseTab<T>& tw) {
     cplx<T>* et = (cplx<T>*)smem;
     const int ne = phase_tab_elems(rp.nphi);
-    const int half = (1 << rp.logP) / 2;
+    const int half = ring_fft_len_k<KIND>(rp) / 2;
     const int n = ne + (rp.logP > 0 ? phase_tab_elems(half) : 0);
     for (int i = threadIdx.x; i < n; i += blockDim.x) et[i] = slot[i];
     E = PhaseTab<T>{et, et + 64, phase_tab_nhi(rp.nphi)};
@@ -57,12 +57,12 @@ __device__ __forceinline__ cplx<T>* ring_tables(unsigned char* smem, const RingP
 // spectrum G (P/2 + 1 entries; G_k = G_{P-k}) are staged in shared memory after
 // the phase tables, once per CTA for all its maps; returns the start of the FFT
 // buffers.
-template <typename T>
+template <int KIND, typename T>
 __device__ __forceinline__ cplx<T>* ring_bluestein_tables(cplx<T>* smem, const RingPair& rp,
                                                           const cplx<T>* __restrict__ gtab,
                                                           const cplx<T>* __restrict__ chirp, const cplx<T>*& Gs,
                                                           const cplx<T>*& cs) {
-    const int half = (1 << rp.logP) / 2 + 1;
+    const int half = ring_fft_len_k<KIND>(rp) / 2 + 1;
     cplx<T>* gsm = smem;
     cplx<T>* csm = smem + half;
     for (int i = threadIdx.x; i < half; i += blockDim.x) gsm[i] = gtab[rp.gtab_off + i];
@@ -72,17 +72,20 @@ __device__ __forceinline__ cplx<T>* ring_bluestein_tables(cplx<T>* smem, const R
     return csm + rp.h + ((half + rp.h) & 1);  // the buffers start 16-byte aligned
 }
 
-// The ring kernels come in two instantiations launched over two ring lists:
-// power-of-two rings (BLUE = false, 3 CTAs per SM for float) and Bluestein rings
-// (BLUE = true, 2 CTAs per SM with 128 registers and the ring's tables in
-// shared memory).  CTA (blockIdx.x, blockIdx.y) runs ring rings[blockIdx.x]
-// for its group of maps.
-template <typename T, bool BLUE>
-constexpr int ring_kernel_ctas() { return BLUE ? 2 : ring_min_ctas<T>(); }
+// The ring kernels come in three instantiations launched over three ring
+// lists: power-of-two rings (KIND 0, 3 CTAs per SM for float), Bluestein rings
+// of length 2^logP (KIND 1, 2 CTAs per SM with 128 registers and the ring's
+// tables in shared memory) and of length 3 * 2^logP (KIND 2, 3072 points: one
+// group of 192 threads, 2 CTAs per SM).  CTA (blockIdx.x, blockIdx.y) runs ring
+// rings[blockIdx.x] for its group of maps.
+template <typename T, int KIND>
+constexpr int ring_kernel_ctas() { return KIND ? 2 : ring_min_ctas<T>(); }
+template <int KIND>
+HPX_HD constexpr int ring_kernel_threads() { return KIND == 2 ? 192 : 256; }
 
 // One CTA per (ring t, group of maps): map[b][ring t] -> F[b][foff_t + m]
-template <typename T, bool BLUE>
-__global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
+template <typename T, int KIND>
+__global__ void __launch_bounds__(ring_kernel_threads<KIND>(), ring_kernel_ctas<T, KIND>())
     k_ring_fwd(const T* __restrict__ map, int nmaps, int maps_per_cta, T* __restrict__ F, int64_t Ftot, Geom geo,
                const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ rtab,
                int rslot, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
@@ -94,13 +97,13 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     const int pr = south ? R - 1 - t : t;
     const RingPair rp = pairs[pr];
     PhaseTab<T> E, tw;
-    cplx<T>* bufs = ring_tables(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
+    cplx<T>* bufs = ring_tables<KIND>(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
     const cplx<T>* Gs = nullptr;
     const cplx<T>* cs = nullptr;
-    if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);
+    if constexpr (KIND > 0) bufs = ring_bluestein_tables<KIND>(bufs, rp, gtab, chirp, Gs, cs);
     __syncthreads();
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
-    const int P = 1 << rp.logP;
+    const int P = ring_fft_len_k<KIND>(rp);
     const int PL = padded_len(P);
     cplx<T>* buf = bufs + (size_t)g * 2 * PL;
     cplx<T>* buf2 = buf + PL;
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
         auto load_next = [&](cplx<T>* dst) {
             if (b + S < b1) ring_load_async(dst, map + (int64_t)(b + S) * np + start, rp.h, lt, tpf);
         };
-        const T mx = ring_forward<BLUE>(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, tw, Gs, cs, E, lt,
+        const T mx = ring_forward<KIND>(cur, other, shift, F + 2 * ((int64_t)b * Ftot + foff), rp, tw, Gs, cs, E, lt,
                                         tpf, g, load_next);
         if (fmax) {
             // per-map max |F| (scale of the FP16 operands); a group is whole warps
@@ -135,8 +138,8 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
 
 // One CTA per (ring t, group of maps): F[b][foff_t + m] -> map[b][ring t]
 // (ref != nullptr: write ref - synthesis)
-template <typename T, bool BLUE>
-__global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
+template <typename T, int KIND>
+__global__ void __launch_bounds__(ring_kernel_threads<KIND>(), ring_kernel_ctas<T, KIND>())
     k_ring_inv(const T* __restrict__ F, int64_t Ftot, T* __restrict__ map, int nmaps, int maps_per_cta, Geom geo,
                const RingPair* __restrict__ pairs, const int* __restrict__ rings, const cplx<T>* __restrict__ rtab,
                int rslot, const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
@@ -148,13 +151,13 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
     const int pr = south ? R - 1 - t : t;
     const RingPair rp = pairs[pr];
     PhaseTab<T> E, tw;
-    cplx<T>* bufs = ring_tables(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
+    cplx<T>* bufs = ring_tables<KIND>(smem_raw, rp, rtab + (size_t)pr * rslot, E, tw);
     const cplx<T>* Gs = nullptr;
     const cplx<T>* cs = nullptr;
-    if constexpr (BLUE) bufs = ring_bluestein_tables(bufs, rp, gtab, chirp, Gs, cs);
+    if constexpr (KIND > 0) bufs = ring_bluestein_tables<KIND>(bufs, rp, gtab, chirp, Gs, cs);
     __syncthreads();
     const int tpf = rp.tpf, S = blockDim.x / tpf, g = threadIdx.x / tpf, lt = threadIdx.x % tpf;
-    const int P = 1 << rp.logP;
+    const int P = ring_fft_len_k<KIND>(rp);
     const int PL = padded_len(P);
     cplx<T>* buf = bufs + (size_t)g * 2 * PL;
     cplx<T>* buf2 = buf + PL;
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(256, ring_kernel_ctas<T, BLUE>())
         auto load_next = [&](cplx<T>* dst) {
             if (b + S < b1) spec_load_async(dst, spec(b + S), rp.mt, lt, tpf);
         };
-        ring_inverse<BLUE>(cur, other, shift, map + (int64_t)b * np + start,
+        ring_inverse<KIND>(cur, other, shift, map + (int64_t)b * np + start,
                            ref ? ref + (int64_t)b * np + start : nullptr, rp, tw, Gs, cs, E, lt, tpf, g, load_next);
     }
 }
@@ -408,7 +411,8 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const RingPair rp = pairs[blockIdx.x];
     if (rp.logh >= 0) return;
-    const int P = 1 << rp.logP, h = rp.h;
+    if (GLOBAL && rp.rad3) return;  // the plan gives lengths 3 * 2^K only to shared-memory builds
+    const int P = ring_fft_len(rp), h = rp.h;
     cplx<double>* buf;
     cplx<double>* buf2;
     cplx<double>* twP = nullptr;
@@ -419,7 +423,16 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
         buf = (cplx<double>*)smem_raw;
         buf2 = buf + padded_len(P);
         twP = buf2 + padded_len(P);
-        load_twiddles(twP, rp.logP, tw64, logPmax);
+        if (rp.rad3) {
+            // twiddles of the length 3 * 2^K, in FP64
+            for (int q = threadIdx.x; q < P / 2; q += blockDim.x) {
+                double sn, cs;
+                sincospi(-2.0 * (double)q / (double)P, &sn, &cs);
+                twP[padi(q)] = {cs, sn};
+            }
+        } else {
+            load_twiddles(twP, rp.logP, tw64, logPmax);
+        }
     }
     for (int j = threadIdx.x; j < P; j += blockDim.x) {
         const int d = j < h ? j : (j > P - h ? P - j : -1);
@@ -435,7 +448,14 @@ __global__ void __launch_bounds__(256) k_chirp_spectra(const RingPair* __restric
     }
     __syncthreads();
     cplx<double>* r;
-    if constexpr (GLOBAL)
+    if (!GLOBAL && rp.rad3) {
+        // one group of fft_tpf(P) threads (whole warps) runs the transform
+        const int tpf = fft_tpf(P);
+        IdentityMap id;
+        if ((int)threadIdx.x < tpf) fft_ring3<double, false>(buf, buf2, rp.logP, FullTw<double>{twP}, threadIdx.x, 0, id, id);
+        __syncthreads();
+        r = (fft3_passes(rp.logP) & 1) ? buf2 : buf;
+    } else if constexpr (GLOBAL)
         r = fft_pow2<double, false>(buf, buf2, rp.logP, StrideTw64{tw64, 1 << (logPmax - rp.logP)}, threadIdx.x,
                                     blockDim.x, 0, IdentityMap{}, IdentityMap{});
     else

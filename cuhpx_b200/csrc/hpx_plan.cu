@@ -92,11 +92,13 @@ struct hpx_plan_s {
     int nmax = 0;   // max nphi
     std::vector<RingPair> h_pairs;
     RingPair* d_pairs = nullptr;
-    // ring lists of the two ring-kernel instantiations: power-of-two rings, then
-    // Bluestein rings (largest first), as ring indices t
+    // ring lists of the three ring-kernel instantiations: power-of-two rings,
+    // Bluestein rings of length 2^K, then of length 3 * 2^K (largest first
+    // within each), as ring indices t
     int* d_rings = nullptr;
-    int n_rings_pow2 = 0, n_rings_blue = 0;
-    int hblue = 0, pblue = 0;  // largest h and FFT length of the Bluestein rings
+    int n_rings_pow2 = 0, n_rings_blue = 0, n_rings_blue3 = 0;
+    int hblue = 0, pblue = 0;    // largest h and FFT length of the Bluestein rings of length 2^K
+    int hblue3 = 0, pblue3 = 0;  // ... and of length 3 * 2^K
     // auxiliary stream and fork/join events: the two ring launches of a
     // transform overlap (the power-of-two rings run on aux); the mutex keeps
     // the record/wait pairs of concurrent callers of one plan apart
@@ -124,7 +126,7 @@ struct hpx_plan_s {
     float wmax = 0.f;            // largest ring weight w_t
     int ring_g = 16;             // maps per ring-FFT CTA (hpx_plan_set_schedule)
     int ring_streams = 2;        // 2: ring launches overlap on the aux stream; 1: serial
-    size_t ring_smem = 0, blue_smem = 0, fwd_smem = 0, inv_smem = 0;
+    size_t ring_smem = 0, blue_smem = 0, blue3_smem = 0, fwd_smem = 0, inv_smem = 0;
     TcPlan tc;  // tensor-core contraction state (mixed precision plans)
 
     // per-kernel event timing (hpx_stats_*)
@@ -226,17 +228,22 @@ int create_typed(hpx_plan_s* P) {
     // chirp spectra computed in FP64 with FP64 twiddles
     int64_t gsize = 0;
     for (auto& rp : P->h_pairs)
-        if (rp.logh < 0) gsize = std::max<int64_t>(gsize, rp.gtab_off + (1ll << rp.logP));
+        if (rp.logh < 0) gsize = std::max<int64_t>(gsize, rp.gtab_off + ring_fft_len(rp));
     if (gsize > 0) {
         cplx<double>* tw64 = nullptr;
         HPX_CUDA_TRY(cudaMalloc(&tw64, (size_t)(Pmax / 2) * sizeof(cplx<double>)));
         k_twiddles<double><<<(Pmax / 2 + 255) / 256, 256>>>(tw64, Pmax);
         HPX_CUDA_TRY(cudaMalloc(&P->d_gtab, (size_t)gsize * sizeof(C)));
         HPX_CUDA_TRY(cudaMalloc(&P->d_chirp, (size_t)gsize * sizeof(C)));
-        size_t sm = (size_t)(2 * padded_len(Pmax) + padded_len(Pmax / 2)) * sizeof(cplx<double>);
+        const int Pbig = std::max(Pmax, P->bufP);  // lengths 3 * 2^K included
+        size_t sm = (size_t)(2 * padded_len(Pbig) + padded_len(Pbig / 2)) * sizeof(cplx<double>);
         int dmax = 0;
         HPX_CUDA_TRY(cudaDeviceGetAttribute(&dmax, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
         cplx<double>* scratch = nullptr;
+        if (P->n_rings_blue3 > 0 && (int)sm > dmax) {
+            cudaFree(tw64);
+            return set_err(HPX_ERR_UNSUPPORTED, "chirp precompute of the 3 * 2^K lengths needs shared memory");
+        }
         if ((int)sm <= dmax) {
             HPX_CUDA_TRY(cudaFuncSetAttribute(k_chirp_spectra<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dmax));
             k_chirp_spectra<T, false><<<P->NP, 256, sm>>>(P->d_pairs, tw64, P->logPmax, (C*)P->d_gtab, (C*)P->d_chirp,
@@ -266,11 +273,16 @@ int create_typed(hpx_plan_s* P) {
     P->ring_smem = ring_smem_elems(P->bufP, P->nmax) * sizeof(C);
     // Bluestein CTAs also hold the ring's chirp and half of its chirp spectrum
     P->blue_smem = P->n_rings_blue ? (ring_smem_elems(P->bufP, P->nmax) + P->pblue / 2 + 2 + P->hblue) * sizeof(C) : 0;
+    // (192-thread CTAs: one group of 192 at 3072 points, 2 x 3072 padded points
+    // of buffers, within ring_smem_elems' 2 x 4096)
+    P->blue3_smem =
+        P->n_rings_blue3 ? (ring_smem_elems(P->bufP, P->nmax) + P->pblue3 / 2 + 2 + P->hblue3) * sizeof(C) : 0;
     P->fwd_smem = fwd_smem_bytes<T>();
     P->inv_smem = inv_smem_bytes<T>(P->L);
     int dev_max = 0;
     HPX_CUDA_TRY(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->device));
-    if ((int)P->ring_smem > dev_max || (int)P->blue_smem > dev_max || (int)P->fwd_smem > dev_max ||
+    if ((int)P->ring_smem > dev_max || (int)P->blue_smem > dev_max || (int)P->blue3_smem > dev_max ||
+        (int)P->fwd_smem > dev_max ||
         (int)P->inv_smem > dev_max)
         return set_err(HPX_ERR_UNSUPPORTED, "nside/lmax too large for the shared-memory kernels of this precision");
     // The attribute is per function, not per plan: always raise it to the device
@@ -278,10 +290,12 @@ int create_typed(hpx_plan_s* P) {
     HPX_CUDA_TRY(cudaStreamCreateWithFlags(&P->aux, cudaStreamNonBlocking));
     HPX_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming));
     HPX_CUDA_TRY(cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
-    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_fwd<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
+    HPX_CUDA_TRY(cudaFuncSetAttribute(k_ring_inv<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_leg_fwd_simt<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_vleg_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
     HPX_CUDA_TRY(cudaFuncSetAttribute(k_vleg_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dev_max));
@@ -747,21 +761,33 @@ void latlon_quadrature(int grid, int n, std::vector<double>& z, std::vector<doub
 int plan_build(hpx_plan_s* P) {
     int64_t goff = 0;
     int logPmax = 1, bufP = 2, mtmax = 0, nmax = 1;
+    // Bluestein length 3 * 2^10 where smaller than the power of two,
+    // for HEALPix grids up to nside 1024 (every length <= 4096: the kernels'
+    // shared-memory budget and the chirp precompute in shared memory)
+    const bool allow_rad3 = P->nside > 0 && P->nside <= 1024;
     for (int p = 0; p < P->NP; ++p) {
         RingPair& rp = P->h_pairs[p];
         rp.h = rp.nphi / 2;
         rp.mt = std::min(P->M, rp.h + 1);
         rp.logh = ilog2_exact(rp.h);
+        rp.rad3 = 0;
         if (rp.logh >= 0) {
             rp.logP = rp.logh;
             rp.gtab_off = -1;
         } else {
             rp.logP = ceil_log2(2 * rp.h - 1);
+            int k3 = 0;
+            while ((3 << k3) < 2 * rp.h - 1) ++k3;
+            if (allow_rad3 && k3 >= kRad3MinK && k3 <= kRad3MaxK && (3 << k3) < (1 << rp.logP) &&
+                fft_tpf(3 << k3) % 32 == 0 && ring_kernel_threads<2>() % fft_tpf(3 << k3) == 0) {
+                rp.rad3 = 1;
+                rp.logP = k3;
+            }
             rp.gtab_off = goff;
-            goff += 1ll << rp.logP;
+            goff += ring_fft_len(rp);
         }
-        const int Pf = 1 << rp.logP;
-        logPmax = std::max(logPmax, std::max(rp.logP, 1));
+        const int Pf = ring_fft_len(rp);
+        if (!rp.rad3) logPmax = std::max(logPmax, std::max(rp.logP, 1));
         bufP = std::max(bufP, Pf);
         // threads per FFT: ~16 points per thread, between one warp and the CTA
         rp.tpf = std::min(256, std::max(32, Pf / 16));
@@ -786,22 +812,30 @@ int plan_build(hpx_plan_s* P) {
     HPX_CUDA_TRY(cudaMalloc(&P->d_pairs, sizeof(RingPair) * P->NP));
     HPX_CUDA_TRY(cudaMemcpy(P->d_pairs, P->h_pairs.data(), sizeof(RingPair) * P->NP, cudaMemcpyHostToDevice));
     {
-        std::vector<int> pw, bl;
+        std::vector<int> pw, bl, b3;
         auto pair_of = [&](int t) -> const RingPair& { return P->h_pairs[t < P->NP ? t : P->R - 1 - t]; };
         for (int t = 0; t < P->R; ++t) {
             const RingPair& rp = pair_of(t);
             if (rp.logh >= 0) {
                 pw.push_back(t);
+            } else if (rp.rad3) {
+                b3.push_back(t);
+                P->hblue3 = std::max(P->hblue3, rp.h);
+                P->pblue3 = std::max(P->pblue3, ring_fft_len(rp));
             } else {
                 bl.push_back(t);
                 P->hblue = std::max(P->hblue, rp.h);
                 P->pblue = std::max(P->pblue, 1 << rp.logP);
             }
         }
-        std::stable_sort(bl.begin(), bl.end(), [&](int a, int b) { return pair_of(a).h > pair_of(b).h; });
+        auto by_h = [&](int a, int b) { return pair_of(a).h > pair_of(b).h; };
+        std::stable_sort(bl.begin(), bl.end(), by_h);
+        std::stable_sort(b3.begin(), b3.end(), by_h);
         P->n_rings_pow2 = (int)pw.size();
         P->n_rings_blue = (int)bl.size();
+        P->n_rings_blue3 = (int)b3.size();
         pw.insert(pw.end(), bl.begin(), bl.end());
+        pw.insert(pw.end(), b3.begin(), b3.end());
         HPX_CUDA_TRY(cudaMalloc(&P->d_rings, sizeof(int) * pw.size()));
         HPX_CUDA_TRY(cudaMemcpy(P->d_rings, pw.data(), sizeof(int) * pw.size(), cudaMemcpyHostToDevice));
     }
@@ -998,7 +1032,8 @@ struct Pipeline {
     // that the two launches and their tails overlap.
     template <typename Pow2, typename Blue>
     void ring_launches(Pow2 pow2, Blue blue) {
-        if (P->n_rings_pow2 && P->n_rings_blue && P->ring_streams == 2) {
+        const bool any_blue = P->n_rings_blue + P->n_rings_blue3 > 0;
+        if (P->n_rings_pow2 && any_blue && P->ring_streams == 2) {
             std::lock_guard<std::mutex> lk(P->fork_mu);
             cudaError_t e = cudaEventRecord(P->ev_fork, st);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(P->aux, P->ev_fork, 0);
@@ -1012,7 +1047,7 @@ struct Pipeline {
             return;
         }
         if (P->n_rings_pow2) pow2(st);
-        if (P->n_rings_blue) blue(st);
+        if (any_blue) blue(st);
     }
 
     // map -> ring spectra F -> folded Legendre operand (spec, or bf16 hi/lo)
@@ -1027,12 +1062,18 @@ struct Pipeline {
             const cplx<T>* rt = (const cplx<T>*)P->d_rtab;
             ring_launches(
                 [&](cudaStream_t s) {
-                    k_ring_fwd<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
+                    k_ring_fwd<T, 0><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
                         map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings, rt, P->rslot, gt, ch, fmax);
                 },
                 [&](cudaStream_t s) {
-                    k_ring_fwd<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
-                        map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot, gt, ch, fmax);
+                    if (P->n_rings_blue)
+                        k_ring_fwd<T, 1><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
+                            map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot, gt,
+                            ch, fmax);
+                    if (P->n_rings_blue3)
+                        k_ring_fwd<T, 2><<<dim3(P->n_rings_blue3, nbk), ring_kernel_threads<2>(), P->blue3_smem, s>>>(
+                            map, nb, g, F, P->Ftot, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2 + P->n_rings_blue,
+                            rt, P->rslot, gt, ch, fmax);
                 });
         }
         Timer tm(P, st, kStFold);
@@ -1057,12 +1098,18 @@ struct Pipeline {
         const cplx<T>* rt = (const cplx<T>*)P->d_rtab;
         ring_launches(
             [&](cudaStream_t s) {
-                k_ring_inv<T, false><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
+                k_ring_inv<T, 0><<<dim3(P->n_rings_pow2, nbk), 256, P->ring_smem, s>>>(
                     F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings, rt, P->rslot, gt, ch, ref);
             },
             [&](cudaStream_t s) {
-                k_ring_inv<T, true><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
-                    F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot, gt, ch, ref);
+                if (P->n_rings_blue)
+                    k_ring_inv<T, 1><<<dim3(P->n_rings_blue, nbk), 256, P->blue_smem, s>>>(
+                        F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2, rt, P->rslot,
+                        gt, ch, ref);
+                if (P->n_rings_blue3)
+                    k_ring_inv<T, 2><<<dim3(P->n_rings_blue3, nbk), ring_kernel_threads<2>(), P->blue3_smem, s>>>(
+                        F, P->Ftot, map, nb, g, P->geo, P->d_pairs, P->d_rings + P->n_rings_pow2 + P->n_rings_blue,
+                        rt, P->rslot, gt, ch, ref);
             });
     }
     void leg_fwd(T* alm, int nb, int accumulate) {

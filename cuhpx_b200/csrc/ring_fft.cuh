@@ -12,8 +12,9 @@
 // a complex sequence of length h = n/2.  If h is a power of two it goes
 // through a Stockham FFT in shared memory (one radix-2/4/8 pass, then radix-16
 // passes, specialised per length), otherwise through Bluestein's chirp-z
-// convolution with a per-ring power-of-two size P >= 2h-1 (the reference pads
-// every ring to 8*nside).  Small rings are transformed by sub-groups of a CTA
+// convolution with a per-ring size P >= 2h-1, a power of two or, where that is
+// smaller (P = 3072), three times one: a twiddle-free radix-12 pass before the
+// radix-16 passes (the reference pads every ring to 8*nside).  Small rings are transformed by sub-groups of a CTA
 // (one warp, two, four or all eight) so that every thread handles ~16 points
 // whatever the ring length.
 //
@@ -43,7 +44,7 @@ struct RingPair {
     int logP;       // log2 of the FFT length actually run (h or the Bluestein size)
     int tpf;        // threads per FFT (32 .. 256)
     int has_south;  // 0 for the equator
-    int pad_;
+    int rad3;       // Bluestein length 3 * 2^logP instead of 2^logP
     int64_t start_n;   // first pixel of the north ring
     int64_t start_s;   // first pixel of the south ring
     int64_t foff_n;    // spectrum offset of the north ring in F[map][.]
@@ -53,6 +54,12 @@ struct RingPair {
     double w;          // quadrature weight of the ring
     double s2;         // sin^2(theta) of the north ring (no cancellation near the poles)
 };
+
+// Length of the FFT a ring runs: h (power-of-two rings), 2^logP or 3 * 2^logP (Bluestein)
+__host__ __device__ __forceinline__ int ring_fft_len(const RingPair& rp) { return (rp.rad3 ? 3 : 1) << rp.logP; }
+// ... for the ring kernels' kinds: 0 power-of-two rings, 1 Bluestein 2^logP, 2 Bluestein 3 * 2^logP
+template <int KIND>
+__device__ __forceinline__ int ring_fft_len_k(const RingPair& rp) { return (KIND == 2 ? 3 : 1) << rp.logP; }
 
 // FFT work buffers are padded by one element every 16 so that the strided
 // Stockham stores of the first pass (stride 16 complex) spread over all banks;
@@ -142,9 +149,62 @@ __device__ __forceinline__ void dft8(cplx<T>* v) {
     v[7] = csub(e3, o3);
 }
 
+// 3-point DFT in registers: X0 = a + (b + c), X1,2 = a - (b + c)/2 -/+ i s (b - c)
+// (forward, s = sin(2 pi/3); the inverse swaps X1 and X2)
+template <typename T, bool INV>
+__device__ __forceinline__ void dft3(cplx<T>* v) {
+    const T s = (T)0.86602540378443864676;
+    const cplx<T> t1 = cadd(v[1], v[2]);
+    const cplx<T> d = cscale(csub(v[1], v[2]), s);
+    const cplx<T> m = {v[0].re - (T)0.5 * t1.re, v[0].im - (T)0.5 * t1.im};
+    v[0] = cadd(v[0], t1);
+    const cplx<T> mi = {m.re + d.im, m.im - d.re};  // m - i d
+    const cplx<T> pi = {m.re - d.im, m.im + d.re};  // m + i d
+    v[1] = INV ? pi : mi;
+    v[2] = INV ? mi : pi;
+}
+
+// 6- and 12-point DFTs in registers as 3 x N2 (N2 = 2, 4) by the prime-factor
+// (Good-Thomas) mapping, which needs no twiddles between the two stages: with
+// n = (N2 n1 + 3 n2) mod N, X[k] = sum_n1 W3^{n1 k} sum_n2 W_N2^{n2 k} x[n], and
+// W3^{n1 k}, W_N2^{n2 k} depend on k only through k mod 3 and k mod N2.
+template <typename T, bool INV, int N2>
+__device__ __forceinline__ void dft3xN2(cplx<T>* v) {
+    constexpr int N = 3 * N2;
+    cplx<T> y[3][N2];
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) y[n1][n2] = v[(N2 * n1 + 3 * n2) % N];
+        if constexpr (N2 == 2) {
+            const cplx<T> a = y[n1][0], b = y[n1][1];
+            y[n1][0] = cadd(a, b);
+            y[n1][1] = csub(a, b);
+        } else {
+            dft4<T, INV>(y[n1][0], y[n1][1], y[n1][2], y[n1][3]);
+        }
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+        cplx<T> t[3] = {y[0][k2], y[1][k2], y[2][k2]};
+        dft3<T, INV>(t);
+        y[0][k2] = t[0];
+        y[1][k2] = t[1];
+        y[2][k2] = t[2];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = y[k % 3][k % N2];
+}
+
 template <typename T, bool INV, int R>
 __device__ __forceinline__ void dftR(cplx<T>* v) {
-    if constexpr (R == 2) {
+    if constexpr (R == 3) {
+        dft3<T, INV>(v);
+    } else if constexpr (R == 6) {
+        dft3xN2<T, INV, 2>(v);
+    } else if constexpr (R == 12) {
+        dft3xN2<T, INV, 4>(v);
+    } else if constexpr (R == 2) {
         const cplx<T> a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
@@ -163,10 +223,8 @@ __device__ __forceinline__ void dftR(cplx<T>* v) {
 template <typename T, int R>
 __device__ __forceinline__ void twiddle_powers(cplx<T> w1, cplx<T>* w) {
     w[1] = w1;
-    if constexpr (R > 2) {
-        w[2] = cmul(w1, w1);
-        w[3] = cmul(w[2], w1);
-    }
+    if constexpr (R > 2) w[2] = cmul(w1, w1);
+    if constexpr (R > 3) w[3] = cmul(w[2], w1);
     if constexpr (R > 4) {
         w[4] = cmul(w[2], w[2]);
         w[5] = cmul(w[4], w1);
@@ -328,34 +386,42 @@ __device__ cplx<T>* fft_pow2(cplx<T>* src, cplx<T>* dst, int logP, const TW& tw,
 HPX_HD constexpr int fft_tpf(int P) { return P / 16 < 32 ? 32 : (P / 16 > 256 ? 256 : P / 16); }
 HPX_HD constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 
-// padded index of i + r * S when the stride S is a multiple of 16 (then the
-// padding of i + rS is the padding of i plus r S/16)
-template <int S>
+// Padding by one element every D: padi is D = 16.  (The pass after the first
+// radix-6/12 pass of the lengths 3 * 2^K reads a buffer padded every 48, which
+// keeps that first pass's stride-R stores and the next pass's loads free of
+// bank conflicts; padded_len(P) covers it.)
+template <int D>
+__device__ __forceinline__ int padd(int i) { return i + i / D; }
+// padded index of i + r * S when the stride S is a multiple of D (then the
+// padding of i + rS is the padding of i plus r S/D)
+template <int S, int D = 16>
 __device__ __forceinline__ int padi_step(int pi, int i, int r) {
-    if constexpr (S % 16 == 0) return pi + r * (S + S / 16);
-    else return padi(i + r * S);
+    if constexpr (S % D == 0) return pi + r * (S + S / D);
+    else return padd<D>(i + r * S);
 }
 
-// ZIN: the input is zero from P/2 on (the first pass then loads and transforms
-// only R/2 of its R inputs); HOUT: only outputs below P/2 are wanted (the last
-// pass forms and stores only those).  Bluestein's convolution has both.
+// ZIN: the input is zero from P/2 on (the first pass then skips the inputs
+// r >= R/2 of its R, which lie at or above P/2); HOUT: only outputs below P/2
+// are wanted (the last pass forms and stores only those).  Bluestein's convolution has both.
 // UNPAD: the last pass stores in natural, unpadded order (its stores are
 // consecutive across a warp, so the padding buys nothing there) -- the inverse
 // ring transform then copies its result out with 16-byte accesses.  UNPIN:
 // likewise the first pass reads an unpadded input (the ring loads then move 16
-// bytes per copy).
+// bytes per copy).  DI, DO: the padding of the input and output buffers.
 template <typename T, bool INV, int R, int NS, int P, int TPF, bool FIRST, bool LAST, bool ZIN, bool HOUT, bool UNPAD,
-          bool UNPIN, typename TW, typename Pre, typename Post>
+          bool UNPIN, int DI = 16, int DO = 16, typename TW, typename Pre, typename Post>
 __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, Pre& pre,
                                             Post& post) {
     constexpr int Q = P / R;
     constexpr int LSTEP = ilog2c(P / (NS * R));
+    // the twiddle step P / (NS R) is a power of two (lengths 2^K and 3 * 2^K, radix 3 first)
+    static_assert(NS == 1 || (NS * R) << LSTEP == P, "twiddle step must be a power of two");
 #pragma unroll
     for (int j0 = 0; j0 < Q; j0 += TPF) {
         const int j = j0 + lt;
         if (Q % TPF != 0 && j >= Q) break;
-        const int k = j & (NS - 1);
-        const int pj = padi(j);
+        const int k = (NS & (NS - 1)) == 0 ? (j & (NS - 1)) : (j % NS);
+        const int pj = padd<DI>(j);
         cplx<T> v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -366,7 +432,7 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
             if constexpr (FIRST && UNPIN)
                 v[r] = src[j + r * Q];
             else
-                v[r] = src[padi_step<Q>(pj, j, r)];
+                v[r] = src[padi_step<Q, DI>(pj, j, r)];
             if constexpr (FIRST) v[r] = pre(j + r * Q, v[r]);
         }
         if constexpr (NS > 1) {
@@ -379,7 +445,7 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
         }
         dftR<T, INV, R>(v);
         const int o = ((j - k) * R) + k;
-        const int po = padi(o);
+        const int po = padd<DO>(o);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (LAST && HOUT && 2 * r >= R) continue;  // o + r NS >= P/2
@@ -388,21 +454,21 @@ __device__ __forceinline__ void fft_pass_ct(const cplx<T>* src, cplx<T>* dst, co
             if constexpr (LAST && UNPAD)
                 dst[o + r * NS] = x;
             else
-                dst[padi_step<NS>(po, o, r)] = x;
+                dst[padi_step<NS, DO>(po, o, r)] = x;
         }
     }
 }
 
 // radix-16 passes NS, 16 NS, ... until the length is P
 template <typename T, bool INV, int P, int TPF, int NS, bool FIRST, bool ZIN, bool HOUT, bool UNPAD, bool UNPIN,
-          typename TW, typename Pre, typename Post>
+          int DI = 16, typename TW, typename Pre, typename Post>
 __device__ __forceinline__ cplx<T>* fft_r16_ct(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
                                                Post& post) {
     if constexpr (NS >= P) {
         return src;
     } else {
         constexpr bool LAST = NS * 16 == P;
-        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, pre, post);
+        fft_pass_ct<T, INV, 16, NS, P, TPF, FIRST, LAST, ZIN, HOUT, UNPAD, UNPIN, DI>(src, dst, tw, lt, pre, post);
         group_sync(TPF, g);
         return fft_r16_ct<T, INV, P, TPF, NS * 16, false, ZIN, HOUT, UNPAD, UNPIN>(dst, src, tw, lt, g, pre, post);
     }
@@ -422,6 +488,31 @@ __device__ __forceinline__ cplx<T>* fft_ct(cplx<T>* src, cplx<T>* dst, const TW&
         return fft_r16_ct<T, INV, P, TPF, 1, true, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
     }
 }
+
+// Length P = 3 * 2^K: one twiddle-free pass of radix 3 * 2^(K mod 4), then
+// radix-16 passes (6, 16, 16 for P = 1536; 12, 16, 16 for P = 3072): as many
+// passes through shared memory as 2048 and 4096 take, over 25% fewer points.
+// The group is fft_tpf(P) = P / 16 threads, which named barriers need to be
+// whole warps.
+template <typename T, bool INV, int K, bool ZIN, bool HOUT, bool UNPAD, bool UNPIN, typename TW, typename Pre,
+          typename Post>
+__device__ __forceinline__ cplx<T>* fft_ct3(cplx<T>* src, cplx<T>* dst, const TW& tw, int lt, int g, Pre& pre,
+                                            Post& post) {
+    constexpr int P = 3 << K, TPF = fft_tpf(P), R3 = 3 << (K & 3);
+    static_assert(TPF % 32 == 0, "an FFT group must be whole warps");
+    static_assert(R3 == 6 || R3 == 12, "first-pass radix");
+    constexpr int D3 = 48;
+    static_assert((P / 16) % D3 == 0, "the second pass's input stride is a multiple of D3");
+    static_assert(P + P / D3 < padded_len(P), "the buffers hold the padding every D3");
+    fft_pass_ct<T, INV, R3, 1, P, TPF, true, false, ZIN, HOUT, UNPAD, UNPIN, 16, D3>(src, dst, tw, lt, pre, post);
+    group_sync(TPF, g);
+    return fft_r16_ct<T, INV, P, TPF, R3, false, ZIN, HOUT, UNPAD, UNPIN, D3>(dst, src, tw, lt, g, pre, post);
+}
+// passes of fft_ct3 (the result is in src when even)
+HPX_HD constexpr int fft3_passes(int K) { return 1 + K / 4; }
+// the length 3 * 2^K the ring kernels run: 3072 (group size 192 threads); a
+// second length would double the kernel's FFT code and its registers
+constexpr int kRad3MinK = 10, kRad3MaxK = 10;
 
 // The ring kernels' FFT: the specialised pass sequence for the group size
 // fft_tpf(P) these kernels use (the generic fft_pow2 otherwise).  ZIN / HOUT
@@ -472,6 +563,17 @@ __device__ __forceinline__ cplx<T>* fft_ring(cplx<T>* src, cplx<T>* dst, int log
     return r;
 }
 
+// fft_ring for the length 3 * 2^K, K = kRad3MinK = kRad3MaxK, with the group
+// size fft_tpf(3 << K)
+template <typename T, bool INV, bool ZIN = false, bool HOUT = false, bool UNPAD = false, bool UNPIN = false,
+          typename TW, typename Pre, typename Post>
+__device__ __forceinline__ cplx<T>* fft_ring3(cplx<T>* src, cplx<T>* dst, int K, const TW tw, int lt, int g, Pre pre,
+                                              Post post) {
+    static_assert(kRad3MinK == kRad3MaxK, "one instantiated length");
+    (void)K;
+    return fft_ct3<T, INV, kRad3MinK, ZIN, HOUT, UNPAD, UNPIN>(src, dst, tw, lt, g, pre, post);
+}
+
 // twP[padi(q)] = e^{-2 pi i q / P}, q < P/2, from the plan's table for Pmax
 // (all threads of the CTA); the table takes padded_len(P/2) entries
 template <typename T>
@@ -483,12 +585,13 @@ __device__ void load_twiddles(cplx<T>* twP, int logP, const cplx<T>* __restrict_
 
 // Complex DFT of length h of buf (natural order, h entries written by this
 // group), forward (e^-) or inverse (e^+); returns the buffer with Z in natural order.
-template <bool BLUE, typename T, typename TW>
+// KIND: 0 power-of-two ring, 1 Bluestein of length 2^logP, 2 of length 3 * 2^logP.
+template <int KIND, typename T, typename TW>
 __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, const TW tw, const cplx<T>* __restrict__ G,
                              const cplx<T>* __restrict__ chirp, bool inv, int lt, int tpf, int g) {
     group_sync(tpf, g);
     IdentityMap id;
-    if constexpr (!BLUE) {
+    if constexpr (KIND == 0) {
         // power-of-two ring
         // (the inverse transform's result in natural unpadded order)
         if (rp.logh == 0) return buf;
@@ -501,7 +604,7 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
         // products ride on the first loads and the last stores of the two FFTs.
         // chirp[0..h) and G[0..P/2] are the ring's tables in shared memory (G is
         // symmetric, G_k = G_{P-k}).
-        const int h = rp.h, P = 1 << rp.logP;
+        const int h = rp.h, P = ring_fft_len_k<KIND>(rp);
         // captures by value: the passes may run in a called (not inlined) function,
         // where a captured reference would be a load from the stack per element
         auto pre = [h, inv, chirp](int j, cplx<T> a) {
@@ -517,11 +620,18 @@ __device__ cplx<T>* ring_dft(cplx<T>* buf, cplx<T>* buf2, const RingPair& rp, co
             return v;
         };
         // a_j = z_j c_j is zero from j = h <= P/2 on, and only Z_k, k < h, is wanted
-        cplx<T>* r = fft_ring<T, false, true, false, false, true>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
-        cplx<T>* o = (r == buf) ? buf2 : buf;
-        // (the inverse transform's result in natural unpadded order)
-        return inv ? fft_ring<T, true, false, true, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc)
-                   : fft_ring<T, true, false, true, false>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
+        if constexpr (KIND == 2) {
+            cplx<T>* r = fft_ring3<T, false, true, false, false, true>(buf, buf2, rp.logP, tw, lt, g, pre, mulG);
+            cplx<T>* o = (r == buf) ? buf2 : buf;
+            return inv ? fft_ring3<T, true, false, true, true>(r, o, rp.logP, tw, lt, g, id, postc)
+                       : fft_ring3<T, true, false, true, false>(r, o, rp.logP, tw, lt, g, id, postc);
+        } else {
+            cplx<T>* r = fft_ring<T, false, true, false, false, true>(buf, buf2, rp.logP, tw, lt, tpf, g, pre, mulG);
+            cplx<T>* o = (r == buf) ? buf2 : buf;
+            // (the inverse transform's result in natural unpadded order)
+            return inv ? fft_ring<T, true, false, true, true>(r, o, rp.logP, tw, lt, tpf, g, id, postc)
+                       : fft_ring<T, true, false, true, false>(r, o, rp.logP, tw, lt, tpf, g, id, postc);
+        }
     }
 }
 
@@ -569,14 +679,14 @@ __device__ __forceinline__ void spec_load_async(cplx<T>* dst, const cplx<T>* Fg,
 // free receives the next map's ring (load_next, asynchronous) while this map's
 // spectrum is formed and stored.  On return cur holds the next input.
 // Returns the largest |re|, |im| this thread wrote.
-template <bool BLUE, typename T, typename Next>
+template <int KIND, typename T, typename Next>
 __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ F, const RingPair& rp,
                           const PhaseTab<T>& tw, const cplx<T>* __restrict__ gtab,
                           const cplx<T>* __restrict__ chirp, const PhaseTab<T>& E, int lt, int tpf, int g,
                           Next load_next) {
     const int h = rp.h;
     cp_async_wait<0>();
-    cplx<T>* Z = ring_dft<BLUE>(cur, other, rp, tw, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
+    cplx<T>* Z = ring_dft<KIND>(cur, other, rp, tw, gtab, chirp, false, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (Z == cur) ? other : cur;
     load_next(freeb);
     T mx = (T)0;
@@ -619,7 +729,7 @@ __device__ T ring_forward(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restri
 // DFT runs there, and the buffer it leaves free receives the next map's
 // spectrum (load_next) while this ring is stored.  On return cur holds the
 // next input.  ref != nullptr: write ref - x (Jacobi residual).
-template <bool BLUE, typename T, typename Next>
+template <int KIND, typename T, typename Next>
 __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __restrict__ x,
                              const T* __restrict__ ref, const RingPair& rp, const PhaseTab<T>& tw,
                              const cplx<T>* __restrict__ gtab, const cplx<T>* __restrict__ chirp,
@@ -648,7 +758,7 @@ __device__ void ring_inverse(cplx<T>*& cur, cplx<T>*& other, int shift, T* __res
         buf[k] = {sum.re - r.im, sum.im + r.re};  // sum + i r (unpadded: the FFT's first pass reads it)
         if (k != 0 && kb != k) buf[kb] = {sum.re + r.im, r.re - sum.im};
     }
-    cplx<T>* z = ring_dft<BLUE>(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
+    cplx<T>* z = ring_dft<KIND>(buf, cur, rp, tw, gtab, chirp, true, lt, tpf, g);  // starts with a group sync
     cplx<T>* freeb = (z == buf) ? cur : buf;
     load_next(freeb);
     // z holds the ring in natural unpadded order: two complex values per

@@ -98,6 +98,35 @@ def test_cfg2_mixed(hpx, cuda, cfg2, prec):
     assert rel(sht0(f32), cfg2["a0"]) < 3e-5
 
 
+# ------------------------------------------------------ Bluestein lengths 3 * 2^k
+@pytest.mark.parametrize("nside", [600, 768])
+def test_bluestein_3x2k_lengths(hpx, cuda, nside):
+    """Rings whose Bluestein convolution runs at 3072 points instead of 4096.
+
+    Polar ring i carries h = 2i complex points and needs a convolution of at
+    least 2h - 1 points: 3072 for i = 513..768.  At nside 600 the rings
+    513..599 and the equatorial rings (h = 1200) run at 3072; at nside 768 the
+    rings 513..767 and the equatorial rings, whose h = 1536 puts 2h - 1 = 3071
+    at the top of the range.  Band-limited maps, 2 of them, L = M = nside + 1,
+    uniform quadrature weights (ring weights exist for powers of two only),
+    against the float64 oracle.
+    """
+    L = nside + 1
+    rng = np.random.default_rng(nside)
+    a = cl_alm(rng, L, 2)
+    f = O.isht_by_m(a, nside)
+    a0 = O.sht_by_m(f, nside, L, L, quad_weights="none")
+    kw = dict(lmax=L, mmax=L, quad_weights="none")
+    with torch.no_grad():
+        at, ft = torch.from_numpy(a).to(cuda), torch.from_numpy(f).to(cuda)
+        assert rel(hpx.iSHTCUDA(nside, **kw)(at), f) < 1e-10
+        assert rel(hpx.SHTCUDA(nside, **kw)(ft), a0) < 1e-10
+        assert rel(hpx.iSHTCUDA(nside, precision="fp32", **kw)(at.to(torch.complex64)), f) < 1e-5
+        assert rel(hpx.SHTCUDA(nside, precision="fp32", **kw)(ft.float()), a0) < 1e-5
+        assert rel(hpx.iSHTCUDA(nside, precision="f16x3", **kw)(at.to(torch.complex64)), f) < 2e-5
+        assert rel(hpx.SHTCUDA(nside, precision="f16x3", refine_iters=0, **kw)(ft.float()), a0) < 2e-5
+
+
 # --------------------------------------------------------------------------- cfg3
 N3, L3 = 1024, 2047
 SPOT = [0, 1, 2, 511, 1023, 2046]
