@@ -50,9 +50,10 @@ def parse():
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged workload (96 maps of mixed nside)")
     ap.add_argument("--no-refined", action="store_true",
                     help="skip the refined variants (1 and 3 Jacobi iterations) of the mixed-precision analysis")
-    ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged", "remap"],
+    ap.add_argument("--workload", default="sht_isht", choices=["sht_isht", "ragged", "remap", "next"],
                     help="sht_isht: the headline step; ragged: 96 maps of mixed nside; remap: NEST -> RING "
-                         "reordering of a batch of maps (with the other layout pairs beside it)")
+                         "reordering of a batch of maps (with the other layout pairs beside it); next: the rows "
+                         "beside the headline (cfg5 loss and regridding with backward, spin-1, healpy packing)")
     ap.add_argument("--accuracy-maps", type=int, default=16)
     ap.add_argument("--spot-maps", type=int, default=2, help="maps checked against the CPU spot oracle")
     return ap.parse_args()
@@ -921,6 +922,119 @@ def run_remap(args):
     return 0
 
 
+def run_next(args):
+    """The rows beside the headline path, timed on one GPU (maps/s, CUDA events,
+    inputs resident, 3 warm-up steps):
+      cfg5_loss   -- loss = sum_lm w_l |a_lm|^2, w_l = 1/(l+1), over the SHT of 16
+                     maps at nside 512, L = M = 1023, forward and backward (FP32
+                     SIMT and f16x3);
+      cfg5_regrid -- Regridding HEALPix nside 256 -> equiangular 512 x 1024 at
+                     L = M = 511, 16 maps, forward, and forward with backward;
+      vector      -- spin-1 VectorSHTCUDA then VectoriSHTCUDA of 16 tangent
+                     fields at nside 256, L = M = 511 (FP32), with the rel-L2 of
+                     the analysis against the FP64 path on 2 fields;
+      healpy      -- dense [64][2048][2048] complex64 a_lm -> healpy packing and
+                     back: GB/s of each against the HBM peak."""
+    import torch
+
+    import cuhpx_b200 as hpx
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    steps, warm = args.steps, max(args.warmup, 3)
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    hbm, _, source = load_peaks()
+    rows = {}
+
+    def rate(fn, maps):
+        ms = time_steps(torch, fn, steps, warm, None, stream) / steps
+        return {"ms_per_step": ms, "maps_per_s": maps / (ms * 1e-3)}
+
+    # cfg5: power-spectrum loss through the SHT, with backward
+    nside, L, B = 512, 1023, 16
+    f = torch.randn((B, 12 * nside * nside), generator=g, device=dev)
+    w = (1.0 / (torch.arange(L, device=dev, dtype=torch.float32) + 1.0))[:, None]
+    rows["cfg5_loss"] = {"config": f"{B} maps, nside {nside}, L = M = {L}, loss + backward"}
+    for prec in ("fp32", "f16x3"):
+        sht = hpx.SHTCUDA(nside, lmax=L, mmax=L, precision=prec)
+        x = f.clone().requires_grad_(True)
+
+        def loss_step():
+            x.grad = None
+            (w * sht(x).abs() ** 2).sum().backward()
+
+        rows["cfg5_loss"][prec] = rate(loss_step, B)
+        del sht
+    # cfg5: regridding HEALPix 256 -> equiangular 512 x 1024, forward and with backward
+    rg = hpx.Regridding(hpx.Grid("healpix", 256), hpx.Grid("equiangular", (512, 1024)), lmax=511, mmax=511)
+    fr = torch.randn((B, 12 * 256 * 256), generator=g, device=dev)
+    xr = fr.clone().requires_grad_(True)
+
+    def regrid_fwd():
+        with torch.no_grad():
+            rg(fr)
+
+    def regrid_bwd():
+        xr.grad = None
+        (rg(xr) ** 2).sum().backward()
+
+    rows["cfg5_regrid"] = {"config": f"{B} maps, HEALPix 256 -> equiangular 512 x 1024, L = M = 511 (FP32)",
+                           "forward": rate(regrid_fwd, B), "forward_backward": rate(regrid_bwd, B)}
+    # spin-1 transforms
+    nside, L = 256, 511
+    vs = hpx.VectorSHTCUDA(nside, lmax=L, mmax=L)
+    vi = hpx.VectoriSHTCUDA(nside, lmax=L, mmax=L)
+    v = torch.randn((B, 2, 12 * nside * nside), generator=g, device=dev)
+
+    def vec_step():
+        with torch.no_grad():
+            vi(vs(v))
+
+    rows["vector"] = {"config": f"{B} tangent fields, nside {nside}, L = M = {L}, analysis then synthesis (FP32)"}
+    rows["vector"].update(rate(vec_step, B))
+    with torch.no_grad():
+        a32 = vs(v[:2])
+        a64 = vs(v[:2].double())
+    rows["vector"]["analysis_rel_l2_vs_fp64"] = float((a32.to(a64.dtype) - a64).abs().pow(2).sum().sqrt()
+                                                      / a64.abs().pow(2).sum().sqrt())
+    del vs, vi, v
+    # healpy packing
+    Lh, Bh = 2048, 64
+    dense = torch.randn((Bh, Lh, Lh), generator=g, device=dev, dtype=torch.complex64)
+    dense = torch.tril(dense)
+    packed = hpx.alm_to_healpy(dense)
+
+    def pack():
+        hpx.alm_to_healpy(dense)
+
+    def unpack():
+        hpx.healpy_to_alm(packed, Lh)
+
+    bytes_pack = dense.numel() * 8 + packed.numel() * 8
+    rp, ru = rate(pack, Bh), rate(unpack, Bh)
+    rows["healpy"] = {"config": f"{Bh} x [{Lh}][{Lh}] complex64 <-> packed [{packed.shape[-1]}]",
+                      "pack": dict(rp, gbs=bytes_pack / (rp["ms_per_step"] * 1e-3) / 1e9,
+                                   frac=bytes_pack / (rp["ms_per_step"] * 1e-3) / 1e9 / hbm),
+                      "unpack": dict(ru, gbs=bytes_pack / (ru["ms_per_step"] * 1e-3) / 1e9,
+                                     frac=bytes_pack / (ru["ms_per_step"] * 1e-3) / 1e9 / hbm),
+                      "peak_source": source}
+    line = {
+        "metric": "rows beside the headline path: cfg5 loss and regridding with backward, spin-1, healpy packing",
+        "value": rows["cfg5_loss"]["f16x3"]["maps_per_s"],
+        "unit": "maps/s (cfg5 loss + backward, f16x3)",
+        "n_gpus": 1,
+        "steps": steps,
+        "warmup": warm,
+        "higher_is_better": True,
+        "data": "synthetic",
+        "rows": rows,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -931,6 +1045,8 @@ def main():
         return run_ragged(args)
     if args.workload == "remap":
         return run_remap(args)
+    if args.workload == "next":
+        return run_next(args)
     return run_gpu(args)
 
 
