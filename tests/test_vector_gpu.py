@@ -75,6 +75,24 @@ def test_vs_oracle(hpx, cuda, nside, L, M):
     assert rel(vi(torch.from_numpy(a).to(cuda, torch.complex64)), ref_f) < 1e-5
 
 
+def test_vs_oracle_nside256(hpx, cuda):
+    """The size the benchmark times (nside 256, L = M = 511): FP64 and FP32
+    analysis and synthesis of 2 tangent fields against the float64 oracle."""
+    nside, L = 256, 511
+    rng = np.random.default_rng(256)
+    f = rng.standard_normal((2, 2, 12 * nside * nside))
+    a = vec_alm(rng, L, L, (2,))
+    vs = hpx.VectorSHTCUDA(nside, lmax=L, mmax=L)
+    vi = hpx.VectoriSHTCUDA(nside, lmax=L, mmax=L)
+    ref_a = V.vsht(f, nside, L, L)
+    ref_f = V.visht(a, nside)
+    with torch.no_grad():
+        assert rel(vs(torch.from_numpy(f).to(cuda)), ref_a) < 1e-10
+        assert rel(vi(torch.from_numpy(a).to(cuda)), ref_f) < 1e-10
+        assert rel(vs(torch.from_numpy(f).float().to(cuda)), ref_a) < 1e-5
+        assert rel(vi(torch.from_numpy(a).to(cuda, torch.complex64)), ref_f) < 1e-5
+
+
 def test_shapes_and_many_chunks(hpx, cuda):
     nside, L = 8, 17
     rng = np.random.default_rng(7)
