@@ -99,8 +99,8 @@ struct hpx_plan_s {
     int n_rings_pow2 = 0, n_rings_blue = 0, n_rings_blue3 = 0;
     int hblue = 0, pblue = 0;    // largest h and FFT length of the Bluestein rings of length 2^K
     int hblue3 = 0, pblue3 = 0;  // ... and of length 3 * 2^K
-    // auxiliary stream and fork/join events: the two ring launches of a
-    // transform overlap (the power-of-two rings run on aux); the mutex keeps
+    // auxiliary stream and fork/join events: the power-of-two ring launch of a
+    // transform runs on aux beside the Bluestein launches; the mutex keeps
     // the record/wait pairs of concurrent callers of one plan apart
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1028,8 +1028,8 @@ struct Pipeline {
     int maps_per_cta_ring() const { return P->ring_g; }
 
     // The power-of-two rings on the plan's auxiliary stream and the Bluestein
-    // rings on st, forked and joined by events (valid under stream capture), so
-    // that the two launches and their tails overlap.
+    // rings (2^K, then 3072 points) on st, forked and joined by events (valid
+    // under stream capture), so that the launches and their tails overlap.
     template <typename Pow2, typename Blue>
     void ring_launches(Pow2 pow2, Blue blue) {
         const bool any_blue = P->n_rings_blue + P->n_rings_blue3 > 0;
